@@ -1,0 +1,159 @@
+/*
+ * nss_b200 -- C ABI of the B200 (sm_100a) BM3D library.
+ *
+ * The reference exposes this path only as a VapourSynth API4 filter,
+ * core.nss_cuda.BM3D (registered in src/cuda/plugin.cpp:76-98 and
+ * src/cuda/bm3d/filter.cpp:118-122, arguments from
+ * src/frontend/bm3d_args.hpp:8-12 plus src/cuda/runtime/context.hpp:17).
+ * This header is the boundary under a VapourSynth shim and under the ctypes
+ * mirror: plain pointers, sizes and status codes, no exceptions, no C++ or
+ * torch types. Each entry point names the reference interface it replaces.
+ *
+ * Threading: every handle may be used from several threads; calls on one
+ * handle serialise internally. nssb_last_error() is per thread.
+ */
+#ifndef NSS_B200_H
+#define NSS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define NSSB_OK 0
+#define NSSB_ERR_ARGUMENT 1 /* creation error; the text is the filter's error message */
+#define NSSB_ERR_CUDA 2     /* a CUDA call failed; context preserved where possible */
+#define NSSB_ERR_RESOURCE 3 /* allocation or memory-limit failure */
+#define NSSB_ERR_STATE 4    /* call not valid for this handle / these inputs */
+#define NSSB_ERR_TIMEOUT 5  /* a bounded device-side wait gave up */
+
+/* Last error text of the calling thread ("" when none). The creation errors
+ * carry the reference's exact messages, e.g. "nss_cuda.BM3D: radius must be
+ * in [0, 16]" (checked_create/mapSetError, src/frontend/validate.hpp:36-52). */
+const char* nssb_last_error(void);
+
+/* Library version string (the plugin's Version(), src/cuda/plugin.cpp:80). */
+const char* nssb_version(void);
+
+/* Device report (the plugin's Backend([device_id]), src/cuda/plugin.cpp:36-72):
+ * writes a one-line JSON object into buf (NUL-terminated, truncated to cap). */
+int nssb_backend_info(int device_id, char* buf, size_t cap);
+
+/* ---- video description (VSVideoInfo / VSVideoFormat fields used by the path) ---- */
+#define NSSB_GRAY 1
+#define NSSB_RGB 2
+#define NSSB_YUV 3
+typedef struct nssb_video_info {
+    int color_family;    /* NSSB_GRAY / NSSB_RGB / NSSB_YUV, 0 = variable */
+    int sample_float;    /* 1 for float samples */
+    int bits_per_sample; /* 32 for the accepted format */
+    int subsampling_w, subsampling_h;
+    int width, height, num_frames;
+} nssb_video_info;
+
+/* ---- creation arguments: the VSMap of the call, key by key, in map order ---- */
+#define NSSB_ARG_INT 1
+#define NSSB_ARG_FLOAT 2
+#define NSSB_ARG_DATA 3
+typedef struct nssb_arg {
+    const char* key;
+    int type;              /* NSSB_ARG_* */
+    int count;             /* elements (1 for data) */
+    const int64_t* ints;   /* NSSB_ARG_INT */
+    const double* floats;  /* NSSB_ARG_FLOAT */
+    const char* data;      /* NSSB_ARG_DATA, NUL-terminated */
+} nssb_arg;
+
+typedef struct nssb_bm3d nssb_bm3d;
+
+/* Argument resolution without a device: every creation check of
+ * nss_cuda.BM3D in the reference's order (checked_create ->
+ * validate_numeric_args and memory_limit_mb, src/frontend/validate.hpp:36-52;
+ * parse_temporal_mode, parse_bm3d, parse_rolling, parse_backend_args,
+ * src/cuda/bm3d/filter.cpp:19-114, src/frontend/bm3d_args.cpp:115-145,
+ * src/frontend/temporal_args.cpp:10-56, src/cuda/runtime/context.cpp:23-41).
+ * ref may be NULL. On success writes the output video info (the legacy
+ * temporal intermediate is (2r+1)*2 planes tall). */
+int nssb_bm3d_check(const nssb_video_info* clip, const nssb_video_info* ref, const nssb_arg* args, int nargs,
+                    nssb_video_info* out_vi);
+
+/* Creation (the `create` of src/cuda/bm3d/filter.cpp:19-114): the checks
+ * above, then device acquisition and device memory for the plan. */
+int nssb_bm3d_create(const nssb_video_info* clip, const nssb_video_info* ref, const nssb_arg* args, int nargs,
+                     nssb_bm3d** out);
+void nssb_bm3d_free(nssb_bm3d* h);
+int nssb_bm3d_output_info(const nssb_bm3d* h, nssb_video_info* out_vi);
+
+/* Input frames that output frame n needs: [*first, *last] of clip (and of
+ * ref when given) -- the arInitial requests of getFrame. */
+int nssb_bm3d_frame_window(const nssb_bm3d* h, int n, int* first, int* last);
+
+/* One frame's planes; strides in elements (float). */
+typedef struct nssb_frame {
+    const float* planes[3];
+    int64_t strides[3];
+} nssb_frame;
+typedef struct nssb_frame_out {
+    float* planes[3];
+    int64_t strides[3];
+} nssb_frame_out;
+#define NSSB_MEM_HOST 0
+#define NSSB_MEM_DEVICE 1
+
+/* Output frame n (the getFrame of the group driver,
+ * src/cuda/common/group_driver.cpp:1803 and :968-1107). clip_frames[i] (and
+ * ref_frames[i], or NULL) are frames first+i, i < count, covering the
+ * window above. memory says where all planes live. With NSSB_MEM_HOST the
+ * copies to and from the device are part of the call. */
+int nssb_bm3d_get_frame(nssb_bm3d* h, int n, const nssb_frame* clip_frames, const nssb_frame* ref_frames, int first,
+                        int count, int memory, nssb_frame_out* out);
+
+/* Kernel accounting of a handle, for measurement (no reference counterpart;
+ * the reference measures through Nsight, tests/cuda/run_ncu.py). With
+ * timing on, the engine brackets its matching, group and finish launches
+ * with CUDA events on its own stream and adds their durations once a frame
+ * completes. flops are the matcher's algorithmic count: 3 * B^2 per
+ * reference-candidate pair (subtract, multiply, add). */
+typedef struct nssb_kernel_stats {
+    int64_t launches;        /* kernels launched by the handle */
+    int64_t match_launches, group_launches, finish_launches;
+    double match_ms, group_ms, finish_ms; /* summed event durations (timing on) */
+    double match_flops;      /* algorithmic matcher flops of the counted launches */
+    double match_pairs;      /* reference-candidate pairs evaluated */
+} nssb_kernel_stats;
+int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stats* out);
+
+/* ---- stage primitives on device memory (the kernels the filter runs) ----
+ * Strides are in elements. stream is a cudaStream_t (NULL = default). */
+
+/* Spatial block matching of every reference of the raster grid
+ * (batch_runner.hpp:17-53; matcher contract src/cpu/bm/matcher.hpp:27-283,
+ * the reference's device form src/cuda/common/match.cu:1685).
+ * pos[j*group+q] = y << 16 | x of match q of reference j (raster order),
+ * -1 past count[j]; dist (may be NULL) the matching SSDs. */
+int nssb_match_spatial(const float* plane, int64_t stride, int width, int height, int block, int step,
+                       int bm_range, int group, int32_t* pos, float* dist, int32_t* count, void* stream);
+
+/* Predictive temporal matching (collect_temporal, matcher.hpp:319-373; device
+ * form match.cu:1707-1757). planes/strides: host arrays of ntemp device
+ * planes; reference slot t0; valid slots [valid_begin, valid_end). slot[j*group+q]
+ * receives the frame slot of each match. */
+int nssb_match_temporal(const float* const* planes, const int64_t* strides, int ntemp, int t0, int valid_begin,
+                        int valid_end, int width, int height, int block, int step, int bm_range, int group,
+                        int ps_num, int ps_range, int32_t* pos, int32_t* slot, float* dist, int32_t* count,
+                        void* stream);
+
+/* One full stage of one plane at radius 0 (process_planes_batched,
+ * src/host/filter_bm3d.cpp:73-339; filter_center, group_driver.cpp:760-856):
+ * match on ref (Wiener) or src (hard threshold, ref NULL), filter every group,
+ * aggregate, finish into dst. sigma is the effective value. */
+int nssb_bm3d_plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int width, int height,
+                          float sigma, int block, int group, int step, int bm_range, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -9,6 +9,9 @@
 #include "bm3d_oracle.h"
 
 #include <math.h>
+#if defined(__AVX2__) && defined(__FMA__)
+#include <immintrin.h>
+#endif
 #include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
@@ -61,32 +64,6 @@ float om_ssd_lanes8(const float* a, ptrdiff_t sa, const float* b, ptrdiff_t sb) 
     return (w[0] + w[2]) + (w[1] + w[3]);
 }
 
-/* SSDs of n consecutive candidates (x0 + c, y), c < n, against a contiguous
- * block*block reference. Each candidate keeps its own row-major FMA chain, so
- * the 16-wide loop (vectorised by the compiler) gives om_ssd's bits. */
-static void ssd_run(const float* refblk, int block, const float* plane, ptrdiff_t stride, int x0, int y, int n,
-                    float* out) {
-    int c0 = 0;
-    for (; c0 + 16 <= n; c0 += 16) {
-        float acc[16];
-        for (int c = 0; c < 16; ++c) acc[c] = 0.f;
-        for (int i = 0; i < block; ++i) {
-            const float* row = plane + (ptrdiff_t)(y + i) * stride + x0 + c0;
-            for (int j = 0; j < block; ++j) {
-                const float r = refblk[i * block + j];
-                for (int c = 0; c < 16; ++c) {
-                    const float d = r - row[j + c];
-                    acc[c] = fmaf(d, d, acc[c]);
-                }
-            }
-        }
-        for (int c = 0; c < 16; ++c) out[c0 + c] = acc[c];
-    }
-    for (; c0 < n; ++c0) {
-        out[c0] = om_ssd(refblk, block, plane + (ptrdiff_t)y * stride + x0 + c0, stride, block);
-    }
-}
-
 /* ------------------------------------------------------------- match order */
 
 /* match_tie_less / match_less (matcher.hpp:27-57) */
@@ -99,12 +76,14 @@ static int tie_less(const om_match* a, const om_match* b) {
     return a->ordinal < b->ordinal;
 }
 
-int om_match_less(const om_match* a, const om_match* b) {
+static inline int match_less(const om_match* a, const om_match* b) {
     const int af = finite_bits(a->dist), bf = finite_bits(b->dist);
     if (af != bf) return af;
     if (af && a->dist != b->dist) return a->dist < b->dist;
     return tie_less(a, b);
 }
+
+int om_match_less(const om_match* a, const om_match* b) { return match_less(a, b); }
 
 /* A top-k set under match_less, kept sorted: the same final set and order as
  * StableTopK (matcher.hpp:59-109) because match_less is a total order on
@@ -117,11 +96,11 @@ typedef struct topk {
 static void topk_add(topk* k, om_match m) {
     if (k->cap <= 0) return;
     if (k->size == k->cap) {
-        if (!om_match_less(&m, &k->s[k->size - 1])) return;
+        if (!match_less(&m, &k->s[k->size - 1])) return;
         --k->size;
     }
     int pos = k->size;
-    while (pos > 0 && om_match_less(&m, &k->s[pos - 1])) {
+    while (pos > 0 && match_less(&m, &k->s[pos - 1])) {
         k->s[pos] = k->s[pos - 1];
         --pos;
     }
@@ -135,7 +114,7 @@ static void topk_adopt(topk* k, int n) {
     for (int i = 1; i < k->size; ++i) {
         om_match m = k->s[i];
         int pos = i;
-        while (pos > 0 && om_match_less(&m, &k->s[pos - 1])) {
+        while (pos > 0 && match_less(&m, &k->s[pos - 1])) {
             k->s[pos] = k->s[pos - 1];
             --pos;
         }
@@ -151,6 +130,55 @@ int om_grid_count(int extent, int block, int step) {
 }
 
 int om_grid_pos(int i, int extent, int block, int step) { return imin(i * step, extent - block); }
+
+/* SSDs of n consecutive candidates of one row of a zero-padded window copy
+ * (buf holds the window rows, each readable for n + 24 + block columns), 24
+ * candidates per pass: each keeps its own row-major FMA chain, the lanes are
+ * independent, so the compiler's vector form gives om_ssd's bits. */
+static void ssd_span(const float* refblk, int block, const float* buf, ptrdiff_t bstride, int n, int nrows,
+                     float* out, int ostride) {
+    /* nrows (<= 4) candidate rows x n candidates; candidate row q starts at buffer row q */
+    for (int c0 = 0; c0 < n; c0 += 24) {
+        float acc[4][24];
+#if defined(__AVX2__) && defined(__FMA__)
+        /* vfmadd is the exactly rounded fma: the same bits as fmaf */
+        __m256 a[4][3];
+        for (int q = 0; q < 4; ++q)
+            for (int v = 0; v < 3; ++v) a[q][v] = _mm256_setzero_ps();
+        for (int i = 0; i < block; ++i) {
+            for (int j = 0; j < block; ++j) {
+                const __m256 r = _mm256_set1_ps(refblk[i * block + j]);
+                for (int q = 0; q < 4; ++q) {
+                    const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
+                    for (int v = 0; v < 3; ++v) {
+                        const __m256 d = _mm256_sub_ps(r, _mm256_loadu_ps(row + 8 * v));
+                        a[q][v] = _mm256_fmadd_ps(d, d, a[q][v]);
+                    }
+                }
+            }
+        }
+        for (int q = 0; q < 4; ++q)
+            for (int v = 0; v < 3; ++v) _mm256_storeu_ps(acc[q] + 8 * v, a[q][v]);
+#else
+        for (int q = 0; q < 4; ++q)
+            for (int c = 0; c < 24; ++c) acc[q][c] = 0.f;
+        for (int i = 0; i < block; ++i)
+            for (int j = 0; j < block; ++j) {
+                const float r = refblk[i * block + j];
+                for (int q = 0; q < 4; ++q) {
+                    const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
+                    for (int c = 0; c < 24; ++c) {
+                        const float d = r - row[c];
+                        acc[q][c] = fmaf(d, d, acc[q][c]);
+                    }
+                }
+            }
+#endif
+        const int m = n - c0 < 24 ? n - c0 : 24;
+        for (int q = 0; q < nrows; ++q)
+            for (int c = 0; c < m; ++c) out[q * ostride + c0 + c] = acc[q][c];
+    }
+}
 
 int om_spatial_match(const float* plane, ptrdiff_t stride, int width, int height, int bx, int by, int block,
                      int bm_range, int group, om_match* out, int lanes8) {
@@ -169,18 +197,35 @@ int om_spatial_match(const float* plane, ptrdiff_t stride, int width, int height
     for (int i = 0; i < block; ++i)
         memcpy(refblk + i * block, plane + (ptrdiff_t)(cy + i) * stride + cx, (size_t)block * sizeof(float));
     const int span = right - left + 1;
-    float dist[2 * 64 + 1];
+    const int rows = bottom - top + block;
+    /* the window rows, zero-padded right and below so every 4-row, 24-wide pass reads in bounds */
+    const ptrdiff_t bstride = span + block + 24 + 8;
+    static __thread float tbuf[(2 * 64 + 32 + 4) * (2 * 64 + 1 + 32 + 24 + 8)];
+    float* buf = tbuf;
+    for (int r = 0; r < rows + 4; ++r) {
+        float* dst = buf + (ptrdiff_t)r * bstride;
+        const int valid = r < rows ? span + block - 1 : 0;
+        if (valid) memcpy(dst, plane + (ptrdiff_t)(top + r) * stride + left, (size_t)valid * sizeof(float));
+        memset(dst + valid, 0, (size_t)(bstride - valid) * sizeof(float));
+    }
+    float dist[4][2 * 64 + 1 + 24];
     for (int y = top; y <= bottom; ++y) {
+        const int q = (y - top) & 3;
+        if (q == 0 && !(lanes8 && block == 8))
+            ssd_span(refblk, block, buf + (ptrdiff_t)(y - top) * bstride, bstride, span, imin(4, bottom - y + 1),
+                     dist[0], 2 * 64 + 1 + 24);
         if (lanes8 && block == 8) {
             for (int c = 0; c < span; ++c)
-                dist[c] = om_ssd_lanes8(refblk, 8, plane + (ptrdiff_t)y * stride + left + c, stride);
-        } else {
-            ssd_run(refblk, block, plane, stride, left, y, span, dist);
+                dist[q][c] = om_ssd_lanes8(refblk, 8, plane + (ptrdiff_t)y * stride + left + c, stride);
         }
         for (int x = left; x <= right; ++x) {
             if (x == cx && y == cy) continue;
+            const float d = dist[q][x - left];
+            /* a finite distance above a full set's worst cannot enter it */
+            if (k.size == k.cap && finite_bits(d) && finite_bits(k.s[k.cap - 1].dist) && d > k.s[k.cap - 1].dist)
+                continue;
             const uint32_t ordinal = (uint32_t)((y - top) * span + (x - left) + 1);
-            topk_add(&k, (om_match){x, y, 0, dist[x - left], ordinal});
+            topk_add(&k, (om_match){x, y, 0, d, ordinal});
         }
     }
     return 1 + k.size;
@@ -349,16 +394,23 @@ static double haar_scale_f64(int n, int j) {
 static void dct_lines(float* base, int n, ptrdiff_t ls, ptrdiff_t ss, int count, int inverse) {
     if (n <= 1) return;
     const float* T = om_dct_table(n);
-    float x[64], y[64];
-    for (int v = 0; v < count; ++v) {
-        float* p = base + v * ls;
-        for (int i = 0; i < n; ++i) x[i] = p[i * ss];
+    /* 8 lines per pass, lane = line: every line keeps its own FMA chain in
+     * index order, so the vector form gives the scalar bits. */
+    for (int v0 = 0; v0 < count; v0 += 8) {
+        const int lanes = count - v0 < 8 ? count - v0 : 8;
+        float x[32 * 8], y[32 * 8];
+        for (int i = 0; i < n; ++i)
+            for (int l = 0; l < 8; ++l) x[i * 8 + l] = l < lanes ? base[(v0 + l) * ls + i * ss] : 0.f;
         for (int o = 0; o < n; ++o) {
-            float acc = 0.f;
-            for (int q = 0; q < n; ++q) acc = fmaf(inverse ? T[q * n + o] : T[o * n + q], x[q], acc);
-            y[o] = acc;
+            float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int q = 0; q < n; ++q) {
+                const float t = inverse ? T[q * n + o] : T[o * n + q];
+                for (int l = 0; l < 8; ++l) acc[l] = fmaf(t, x[q * 8 + l], acc[l]);
+            }
+            for (int l = 0; l < 8; ++l) y[o * 8 + l] = acc[l];
         }
-        for (int i = 0; i < n; ++i) p[i * ss] = y[i];
+        for (int i = 0; i < n; ++i)
+            for (int l = 0; l < lanes; ++l) base[(v0 + l) * ls + i * ss] = y[i * 8 + l];
     }
 }
 
@@ -372,24 +424,32 @@ static void dct2_cube(float* c, int group, int block, int inverse) {
  * difference high); forward scales last, inverse first. */
 static void haar_lines(float* base, int n, ptrdiff_t ls, ptrdiff_t ss, int count, int inverse) {
     if (n <= 1) return;
-    for (int v = 0; v < count; ++v) {
-        float* p = base + v * ls;
-        if (inverse) {
-            for (int j = 0; j < n; ++j) p[j * ss] = p[j * ss] * om_haar_scale(n, j);
-            for (int h = n / 2; h >= 1; h >>= 1)
-                for (int i = 0; i < n; i += 2 * h) {
+    /* level by level over all lines at once: the same operations per sample */
+    if (inverse) {
+        for (int j = 0; j < n; ++j) {
+            const float f = om_haar_scale(n, j);
+            for (int v = 0; v < count; ++v) base[v * ls + j * ss] = base[v * ls + j * ss] * f;
+        }
+        for (int h = n / 2; h >= 1; h >>= 1)
+            for (int i = 0; i < n; i += 2 * h)
+                for (int v = 0; v < count; ++v) {
+                    float* p = base + v * ls;
                     const float a = p[i * ss], b = p[(i + h) * ss];
                     p[i * ss] = a + b;
                     p[(i + h) * ss] = a - b;
                 }
-        } else {
-            for (int h = 1; h < n; h <<= 1)
-                for (int i = 0; i < n; i += 2 * h) {
+    } else {
+        for (int h = 1; h < n; h <<= 1)
+            for (int i = 0; i < n; i += 2 * h)
+                for (int v = 0; v < count; ++v) {
+                    float* p = base + v * ls;
                     const float a = p[i * ss], b = p[(i + h) * ss];
                     p[i * ss] = a + b;
                     p[(i + h) * ss] = a - b;
                 }
-            for (int j = 0; j < n; ++j) p[j * ss] = p[j * ss] * om_haar_scale(n, j);
+        for (int j = 0; j < n; ++j) {
+            const float f = om_haar_scale(n, j);
+            for (int v = 0; v < count; ++v) base[v * ls + j * ss] = base[v * ls + j * ss] * f;
         }
     }
 }
@@ -586,6 +646,13 @@ static void finish_plane(float* dst, ptrdiff_t dstride, const float* num, const 
 
 int om_bm3d_plane(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width, int height,
                   const om_stage* st, int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts) {
+    return om_bm3d_plane_matched(src, sstride, ref, rstride, NULL, 0, width, height, st, wiener, dst, dstride, matches,
+                                 counts);
+}
+
+int om_bm3d_plane_matched(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride,
+                          const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st,
+                          int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts) {
     if (st->sigma == 0.f) {
         for (int y = 0; y < height; ++y) memcpy(dst + y * dstride, src + y * sstride, (size_t)width * sizeof(float));
         return 0;
@@ -600,8 +667,8 @@ int om_bm3d_plane(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff
         free(cube);
         return -1;
     }
-    const float* match_src = wiener ? ref : src;
-    const ptrdiff_t match_stride = wiener ? rstride : sstride;
+    const float* match_src = match ? match : (wiener ? ref : src);
+    const ptrdiff_t match_stride = match ? mstride : (wiener ? rstride : sstride);
     pass_ctx c = {&src, &sstride, wiener ? &ref : NULL, &rstride, width, height, st, wiener,
                   num, num + plane, 1, 0, 0};
     const int nx = om_grid_count(width, block, st->step), ny = om_grid_count(height, block, st->step);

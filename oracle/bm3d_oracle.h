@@ -95,6 +95,12 @@ double om_filter_group_f64(double* cube, const double* ref, int group, int block
 int om_bm3d_plane(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width, int height,
                   const om_stage* st, int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts);
 
+/* The same with the groups matched on another plane (CBM3D, filter_bm3d.cpp:
+ * 451-486: every plane filtered with plane 0's groups); match NULL = as above. */
+int om_bm3d_plane_matched(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride,
+                          const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st,
+                          int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts);
+
 /* Radius > 0, one plane of a whole clip: each centre c matches predictively
  * over its 2r+1 slots (temporal.hpp:19-21), filters and adds to num/den
  * slices of its target frames; each frame is then reduced over its centres

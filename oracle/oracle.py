@@ -64,6 +64,10 @@ def lib():
         L.om_bm3d_plane.restype = C.c_int
         L.om_bm3d_plane.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int, C.POINTER(Stage), C.c_int,
                                     fp, C.c_ssize_t, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.om_bm3d_plane_matched.restype = C.c_int
+        L.om_bm3d_plane_matched.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int,
+                                            C.POINTER(Stage), C.c_int, fp, C.c_ssize_t, C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int32)]
         L.om_bm3d_plane_clip.restype = C.c_int
         L.om_bm3d_plane_clip.argtypes = [C.POINTER(fp), C.POINTER(fp), C.c_int, C.c_int, C.c_int, C.c_ssize_t,
                                          C.POINTER(Stage), C.c_int, C.c_int, C.POINTER(fp)]
@@ -175,6 +179,27 @@ def bm3d_plane(src, st: Stage, ref=None, want_matches=False):
     if want_matches:
         return dst, matches, counts
     return dst
+
+
+def bm3d_planes_chroma(planes, st: Stage, refs=None):
+    """CBM3D: groups matched on plane 0 (of refs when given) filter every plane."""
+    ps = [_f32(p) for p in planes]
+    rs = [_f32(p) for p in refs] if refs is not None else None
+    h, w = ps[0].shape
+    match = rs[0] if rs is not None else ps[0]
+    outs = []
+    for c, p in enumerate(ps):
+        dst = np.empty_like(p)
+        r = rs[c] if rs is not None else None
+        if st.sigma == 0.0:
+            outs.append(p.copy())
+            continue
+        rc = lib().om_bm3d_plane_matched(_fp(p), w, _fp(r) if r is not None else None, w, _fp(match), w, w, h,
+                                         C.byref(st), int(r is not None), _fp(dst), w, None, None)
+        if rc != 0:
+            raise RuntimeError("oracle plane pass failed")
+        outs.append(dst)
+    return outs
 
 
 def bm3d_plane_two_stage(src, basic: Stage, final: Stage):

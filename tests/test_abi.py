@@ -1,0 +1,49 @@
+"""The C-ABI library loads without a GPU and exports every entry point the
+public header declares; calls that need no device behave."""
+import ctypes as C
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = set()
+    for header in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(nssb_[a-z_0-9]+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ("nssb_last_error", "nssb_bm3d_create", "nssb_bm3d_get_frame", "nssb_match_spatial",
+              "nssb_bm3d_plane_stage", "nssb_bm3d_check"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(nssb):
+    lib = nssb.lib()
+    missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_error_without_device(nssb):
+    assert "sm_100a" in nssb.version()
+    assert nssb.last_error() == ""
+
+
+def test_create_without_device_is_a_creation_error(nssb):
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    vi = nssb.format_info("GRAYS", 48, 40, 4)
+    clip = nssb.Clip([(None,)] * 4, vi)
+    try:
+        nssb.BM3D(clip)
+    except nssb.Error as e:
+        assert str(e).startswith("nss_cuda.BM3D: no CUDA device available")
+    else:
+        raise AssertionError("creation without a device must fail")

@@ -1,0 +1,180 @@
+"""GPU parity of the CUDA path against the CPU oracle (through the C ABI).
+
+- Matching: the device groups equal the oracle's exactly (positions, order,
+  counts) and the distances are bit-identical: both use one FMA chain per
+  candidate in row-major order. Near-ties therefore cannot flip.
+- Stages and frames: PSNR of the device output against the oracle's, with
+  the reference's own contract floor of 60 dB (tests/data/cuda_tolerances_v1.json)
+  and a max-abs bound; run-to-run bit identity (fixed-point sums).
+"""
+import ctypes as C
+import importlib
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+MIN_PSNR = 60.0
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def synth():
+    return importlib.import_module("vapoursynth-nssfactory_b200.synth")
+
+
+def to_dev(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def gpu_match(nssb, plane_np, block, step, rng_, group, dev):
+    h, w = plane_np.shape
+    d = to_dev(plane_np, dev)
+    nx = (w - block + step - 1) // step + 1
+    ny = (h - block + step - 1) // step + 1
+    pos = torch.full((nx * ny, group), -7, dtype=torch.int32, device=dev)
+    dist = torch.zeros((nx * ny, group), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(nx * ny, dtype=torch.int32, device=dev)
+    nssb.check(nssb.lib().nssb_match_spatial(d.data_ptr(), w, w, h, block, step, rng_, group, pos.data_ptr(),
+                                             dist.data_ptr(), cnt.data_ptr(), None))
+    torch.cuda.synchronize()
+    return pos.cpu().numpy(), dist.cpu().numpy(), cnt.cpu().numpy()
+
+
+SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 7), (12, 6, 8, 5),
+          (2, 2, 4, 4), (1, 1, 2, 3), (32, 16, 4, 3), (8, 3, 64, 7), (8, 8, 1, 9), (4, 3, 16, 12)]
+
+
+@pytest.mark.parametrize("block,step,group,rng_", SHAPES)
+def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_):
+    noisy, _ = synth.gray_frame(5, 61, 47, sigma=10)
+    pos, dist, cnt = gpu_match(nssb, noisy, block=block, step=step, rng_=rng_, group=group, dev=dev)
+    st = oracle.stage(oracle.effective_sigma(10.0), block=block, group=group, step=step, bm_range=rng_)
+    _, want, wcnt = oracle.bm3d_plane(noisy, st, want_matches=True)
+    assert np.array_equal(cnt, wcnt)
+    assert np.array_equal(pos, want)
+    # distances bit-identical with the oracle's SSD
+    nx = (61 - block + step - 1) // step + 1
+    for j in range(0, pos.shape[0], max(1, pos.shape[0] // 23)):
+        bx, by = min((j % nx) * step, 61 - block), min((j // nx) * step, 47 - block)
+        om = oracle.spatial_match(noisy, bx, by, block, rng_, group)
+        assert [m[3] for m in om] == [float(v) for v in dist[j, :len(om)]]
+
+
+def test_match_exact_ties(nssb, oracle, dev):
+    # piecewise-constant image: exact distance ties resolve by (y, x) (test_cuda_match.cpp:33-46)
+    img = np.kron(np.array([[0.25, 0.5], [0.75, 0.25]], np.float32), np.ones((16, 20), np.float32))
+    pos, _, cnt = gpu_match(nssb, img, block=8, step=4, rng_=9, group=16, dev=dev)
+    st = oracle.stage(0.01, block=8, group=16, step=4, bm_range=9)
+    _, want, wcnt = oracle.bm3d_plane(img, st, want_matches=True)
+    assert np.array_equal(pos, want) and np.array_equal(cnt, wcnt)
+
+
+def test_match_nonfinite(nssb, oracle, dev):
+    rng = np.random.default_rng(1)
+    img = rng.uniform(0, 1, (40, 48)).astype(np.float32)
+    img[10, 11] = np.nan
+    img[30, 40] = np.inf
+    pos, _, cnt = gpu_match(nssb, img, block=8, step=8, rng_=9, group=8, dev=dev)
+    with np.errstate(all="ignore"):
+        st = oracle.stage(0.01)
+        _, want, wcnt = oracle.bm3d_plane(img, st, want_matches=True)
+    assert np.array_equal(cnt, wcnt)
+    assert np.array_equal(pos, want)
+
+
+def gpu_stage(nssb, src, ref, st, dev):
+    h, w = src.shape
+    s = to_dev(src, dev)
+    r = to_dev(ref, dev) if ref is not None else None
+    out = torch.empty_like(s)
+    nssb.check(nssb.lib().nssb_bm3d_plane_stage(s.data_ptr(), r.data_ptr() if r is not None else None,
+                                                out.data_ptr(), w, w, h, st.sigma, st.block, st.group, st.step,
+                                                st.bm_range, None))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+STAGES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (16, 8, 16, 7), (12, 6, 8, 5), (2, 2, 4, 4), (1, 1, 2, 3),
+          (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4)]
+
+
+@pytest.mark.parametrize("block,step,group,rng_", STAGES)
+@pytest.mark.parametrize("wiener", [False, True])
+def test_stage_vs_oracle(nssb, oracle, synth, dev, block, step, group, rng_, wiener):
+    noisy, clean = synth.gray_frame(9, 96, 80, sigma=20)
+    st = oracle.stage(oracle.effective_sigma(20.0), block=block, group=group, step=step, bm_range=rng_)
+    ref = oracle.bm3d_plane(noisy, st) if wiener else None
+    want = oracle.bm3d_plane(noisy, st, ref=ref)
+    got = gpu_stage(nssb, noisy, ref, st, dev)
+    p = oracle.psnr(got, want)
+    assert p >= MIN_PSNR, p
+    assert np.max(np.abs(got - want)) < 1e-3
+    assert np.array_equal(got, gpu_stage(nssb, noisy, ref, st, dev))  # run-to-run identical
+
+
+def test_frame_api_two_stage_yuv420(nssb, oracle, synth, dev):
+    frames = synth.yuv420_clip(3, 128, 96, frames=2, sigma=5)
+    clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
+    node = nssb.BM3D(clip, sigma=5, final=1)
+    s = oracle.stage(oracle.effective_sigma(5.0))
+    for n in range(2):
+        got = node.get_frame(n)
+        want = [oracle.bm3d_plane_two_stage(p, s, s)[0] for p in frames[n]]
+        assert oracle.psnr(list(got), want) >= MIN_PSNR
+    node.close()
+
+
+def test_frame_api_device_resident_equals_host(nssb, synth, dev):
+    frames = synth.yuv420_clip(4, 96, 64, frames=1, sigma=10)
+    host = nssb.BM3D(nssb.Clip.from_frames(frames, nssb.YUV, 1, 1), sigma=10, final=1).get_frame(0)
+    dframes = [tuple(to_dev(p, dev) for p in f) for f in frames]
+    devout = nssb.BM3D(nssb.Clip.from_frames(dframes, nssb.YUV, 1, 1), sigma=10, final=1).get_frame(0)
+    for a, b in zip(host, devout):
+        assert np.array_equal(a, b.cpu().numpy())
+
+
+def test_frame_api_ref_and_sigma_zero(nssb, oracle, synth, dev):
+    frames = synth.yuv420_clip(6, 96, 64, frames=1, sigma=10)
+    clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
+    basic = nssb.BM3D(clip, sigma=[10, 0, 7]).get_frame(0)
+    assert np.array_equal(basic[1], frames[0][1])  # sigma 0 copies the plane
+    refclip = nssb.Clip.from_frames([basic], nssb.YUV, 1, 1)
+    final = nssb.BM3D(clip, ref=refclip, sigma=[10, 0, 7]).get_frame(0)
+    both = nssb.BM3D(clip, sigma=[10, 0, 7], final=1).get_frame(0)
+    for a, b in zip(final, both):  # final=1 is the two calls (bm3d_args.cpp:161-196)
+        assert np.array_equal(a, b)
+    s = oracle.stage(oracle.effective_sigma(10.0))
+    want = oracle.bm3d_plane_two_stage(frames[0][0], s, s)[0]
+    assert oracle.psnr(final[0], want) >= MIN_PSNR
+
+
+def test_frame_api_chroma(nssb, oracle, synth, dev):
+    rng = np.random.default_rng(2)
+    y, _ = synth.gray_frame(8, 64, 48, sigma=10)
+    u = (y * 0.3 + rng.normal(0, 0.02, y.shape)).astype(np.float32)
+    v = (0.5 - y * 0.2 + rng.normal(0, 0.02, y.shape)).astype(np.float32)
+    clip = nssb.Clip.from_frames([(y, u, v)], nssb.YUV, 0, 0)
+    got = nssb.BM3D(clip, sigma=[10, 6, 6], chroma=1).get_frame(0)
+    # plane 0 exactly as without chroma; every plane filtered with the plane-0 groups
+    alone = nssb.BM3D(nssb.Clip.from_frames([(y,)], nssb.GRAY), sigma=10).get_frame(0)
+    assert np.array_equal(got[0], alone[0])
+    for c, sg in enumerate((10.0, 6.0, 6.0)):
+        st = oracle.stage(oracle.effective_sigma(sg))
+        want = oracle.bm3d_planes_chroma([y, u, v], st)[c]
+        assert oracle.psnr(got[c], want) >= MIN_PSNR
+    # two-stage CBM3D: plane 0 of the basic estimate guides the Wiener stage
+    both = nssb.BM3D(clip, sigma=[10, 6, 6], chroma=1, final=1).get_frame(0)
+    for c, sg in enumerate((10.0, 6.0, 6.0)):
+        st = oracle.stage(oracle.effective_sigma(sg))
+        basic = oracle.bm3d_planes_chroma([y, u, v], st)
+        want = oracle.bm3d_planes_chroma([y, u, v], st, refs=basic)[c]
+        assert oracle.psnr(both[c], want) >= MIN_PSNR

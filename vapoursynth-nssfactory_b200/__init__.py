@@ -1,0 +1,309 @@
+"""Python mirror of ``core.nss_cuda.BM3D`` over the C ABI of ``libnss_b200.so``.
+
+The reference exposes BM3D as a VapourSynth API4 filter (src/cuda/plugin.cpp:76-98,
+src/cuda/bm3d/filter.cpp:19-122). This module offers the same call for users
+and tests without VapourSynth: ``BM3D(clip, ref=None, **args)`` with the same
+argument names, defaults and creation errors (raised as :class:`Error` with
+the filter's exact text), returning a node whose ``get_frame(n)`` renders a
+frame on the GPU. Clips are lists of frames; a frame is a tuple of 2-D float32
+planes (numpy arrays in host memory, or torch CUDA tensors for device-resident
+frames).
+
+There is no CPU path: without the library, or without a B200, calls fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Sequence
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libnss_b200.so"
+
+# kBm3dSignature (src/frontend/bm3d_args.hpp:8-12) + kBackendSignature (src/cuda/runtime/context.hpp:17)
+SIGNATURE = (
+    "clip:vnode;ref:vnode:opt;sigma:float[]:opt;block_size:int[]:opt;group_size:int[]:opt;"
+    "block_step:int[]:opt;bm_range:int[]:opt;radius:int:opt;ps_num:int[]:opt;ps_range:int[]:opt;chroma:int:opt;"
+    "final:int:opt;sigma_basic:float[]:opt;block_size_basic:int[]:opt;group_size_basic:int[]:opt;"
+    "temporal_mode:data:opt;rolling_chunk:int:opt;rolling_cache_chunks:int:opt;rolling_cache_limit:int:opt;"
+    "memory_limit_mb:int:opt;device_id:int:opt;num_streams:int:opt;"
+)
+
+GRAY, RGB, YUV = 1, 2, 3
+OK, ERR_ARGUMENT, ERR_CUDA, ERR_RESOURCE, ERR_STATE, ERR_TIMEOUT = range(6)
+MEM_HOST, MEM_DEVICE = 0, 1
+ARG_INT, ARG_FLOAT, ARG_DATA = 1, 2, 3
+
+
+class Error(Exception):
+    """A filter error (the text VapourSynth would report as vs.Error)."""
+
+
+def parse_signature(sig: str = SIGNATURE):
+    out = {}
+    for item in filter(None, sig.split(";")):
+        name, kind, *flags = item.split(":")
+        out[name] = (kind.rstrip("[]"), kind.endswith("[]"), "opt" in flags)
+    return out
+
+
+ARGS = parse_signature()
+
+
+class VideoInfo(C.Structure):
+    _fields_ = [("color_family", C.c_int), ("sample_float", C.c_int), ("bits_per_sample", C.c_int),
+                ("subsampling_w", C.c_int), ("subsampling_h", C.c_int), ("width", C.c_int), ("height", C.c_int),
+                ("num_frames", C.c_int)]
+
+    def planes(self) -> int:
+        return 1 if self.color_family == GRAY else 3
+
+    def plane_shape(self, p: int):
+        return (self.height >> (self.subsampling_h if p else 0), self.width >> (self.subsampling_w if p else 0))
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Arg(C.Structure):
+    _fields_ = [("key", C.c_char_p), ("type", C.c_int), ("count", C.c_int), ("ints", C.POINTER(C.c_int64)),
+                ("floats", C.POINTER(C.c_double)), ("data", C.c_char_p)]
+
+
+class Frame(C.Structure):
+    _fields_ = [("planes", C.c_void_p * 3), ("strides", C.c_int64 * 3)]
+
+
+class FrameOut(C.Structure):
+    _fields_ = [("planes", C.c_void_p * 3), ("strides", C.c_int64 * 3)]
+
+
+class KernelStats(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("match_launches", C.c_int64), ("group_launches", C.c_int64),
+                ("finish_launches", C.c_int64), ("match_ms", C.c_double), ("group_ms", C.c_double),
+                ("finish_ms", C.c_double), ("match_flops", C.c_double), ("match_pairs", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (or __graft_entry__.build())")
+        L = C.CDLL(str(LIB_PATH))
+        L.nssb_last_error.restype = C.c_char_p
+        L.nssb_version.restype = C.c_char_p
+        L.nssb_backend_info.argtypes = [C.c_int, C.c_char_p, C.c_size_t]
+        L.nssb_bm3d_check.argtypes = [C.POINTER(VideoInfo), C.POINTER(VideoInfo), C.POINTER(Arg), C.c_int,
+                                      C.POINTER(VideoInfo)]
+        L.nssb_bm3d_create.argtypes = [C.POINTER(VideoInfo), C.POINTER(VideoInfo), C.POINTER(Arg), C.c_int,
+                                       C.POINTER(C.c_void_p)]
+        L.nssb_bm3d_free.argtypes = [C.c_void_p]
+        L.nssb_bm3d_free.restype = None
+        L.nssb_bm3d_output_info.argtypes = [C.c_void_p, C.POINTER(VideoInfo)]
+        L.nssb_bm3d_frame_window.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.nssb_bm3d_get_frame.argtypes = [C.c_void_p, C.c_int, C.POINTER(Frame), C.POINTER(Frame), C.c_int, C.c_int,
+                                          C.c_int, C.POINTER(FrameOut)]
+        L.nssb_bm3d_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(KernelStats)]
+        L.nssb_match_spatial.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nssb_match_temporal.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nssb_bm3d_plane_stage.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                            C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().nssb_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise Error(last_error())
+
+
+def video_info(family: int, width: int, height: int, num_frames: int, ss_w: int = 0, ss_h: int = 0) -> VideoInfo:
+    return VideoInfo(family, 1, 32, ss_w, ss_h, width, height, num_frames)
+
+
+FORMATS = {
+    "GRAYS": (GRAY, 0, 0),
+    "RGBS": (RGB, 0, 0),
+    "YUV444PS": (YUV, 0, 0),
+    "YUV420PS": (YUV, 1, 1),
+    "YUV422PS": (YUV, 1, 0),
+}
+
+
+def format_info(name: str, width: int, height: int, num_frames: int) -> VideoInfo:
+    fam, sw, sh = FORMATS[name]
+    return video_info(fam, width, height, num_frames, sw, sh)
+
+
+class _ArgBuffer:
+    """The call's arguments as nssb_arg entries (types as VapourSynth coerces them)."""
+
+    def __init__(self, kwargs: dict):
+        self.keep = []
+        entries = []
+        for key, value in kwargs.items():
+            if key not in ARGS:
+                raise Error(f"BM3D: Function does not take argument(s) named {key}")
+            kind, is_array, _ = ARGS[key]
+            if value is None:
+                continue
+            vals = list(value) if isinstance(value, (list, tuple)) else [value]
+            if not is_array and len(vals) != 1:
+                raise Error(f"BM3D: Argument '{key}' is not an array")
+            if kind == "int":
+                if any(isinstance(v, float) for v in vals):
+                    raise Error(f"BM3D: Argument '{key}' is not of type int")
+                arr = (C.c_int64 * len(vals))(*[int(v) for v in vals])
+                self.keep.append(arr)
+                entries.append(Arg(key.encode(), ARG_INT, len(vals), arr, None, None))
+            elif kind == "float":
+                arr = (C.c_double * len(vals))(*[float(v) for v in vals])
+                self.keep.append(arr)
+                entries.append(Arg(key.encode(), ARG_FLOAT, len(vals), None, arr, None))
+            elif kind == "data":
+                data = vals[0].encode() if isinstance(vals[0], str) else bytes(vals[0])
+                self.keep.append(data)
+                entries.append(Arg(key.encode(), ARG_DATA, 1, None, None, data))
+            else:
+                raise Error(f"BM3D: Argument '{key}' has an unsupported type")
+        self.array = (Arg * max(1, len(entries)))(*entries)
+        self.count = len(entries)
+
+
+def check_args(clip_vi: VideoInfo, ref_vi: VideoInfo | None = None, **kwargs) -> VideoInfo:
+    """Creation checks only (no device): the output video info, or Error."""
+    args = _ArgBuffer(kwargs)
+    out = VideoInfo()
+    check(lib().nssb_bm3d_check(C.byref(clip_vi), C.byref(ref_vi) if ref_vi is not None else None, args.array,
+                                args.count, C.byref(out)))
+    return out
+
+
+@dataclass
+class Clip:
+    """A clip: frames (each a tuple of 2-D float32 planes) and its format."""
+
+    frames: Sequence
+    vi: VideoInfo
+
+    @staticmethod
+    def from_frames(frames, family: int = GRAY, ss_w: int = 0, ss_h: int = 0) -> "Clip":
+        frames = [tuple(f) if isinstance(f, (tuple, list)) else (f,) for f in frames]
+        h, w = frames[0][0].shape
+        return Clip(frames, video_info(family, w, h, len(frames), ss_w, ss_h))
+
+    @property
+    def device(self) -> bool:
+        p = self.frames[0][0]
+        return hasattr(p, "is_cuda") and p.is_cuda
+
+
+def _plane_ptr(p):
+    if hasattr(p, "data_ptr"):
+        assert p.dtype.__str__() == "torch.float32" and p.stride(1) == 1
+        return p.data_ptr(), p.stride(0)
+    assert p.dtype == np.float32 and p.strides[1] == 4
+    return p.ctypes.data, p.strides[0] // 4
+
+
+class Node:
+    """A created BM3D filter; frames render on the GPU."""
+
+    def __init__(self, clip: Clip, ref: Clip | None, kwargs: dict):
+        self.clip, self.ref = clip, ref
+        args = _ArgBuffer(kwargs)
+        h = C.c_void_p()
+        check(lib().nssb_bm3d_create(C.byref(clip.vi), C.byref(ref.vi) if ref is not None else None, args.array,
+                                     args.count, C.byref(h)))
+        self.handle = h
+        self.vi = VideoInfo()
+        check(lib().nssb_bm3d_output_info(self.handle, C.byref(self.vi)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().nssb_bm3d_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def stats(self, enable_timing: bool, reset: bool) -> KernelStats:
+        """Kernel accounting since the last reset; turns event timing on or off."""
+        st = KernelStats()
+        check(lib().nssb_bm3d_stats(self.handle, int(enable_timing), int(reset), C.byref(st)))
+        return st
+
+    def frame_window(self, n: int):
+        a, b = C.c_int(), C.c_int()
+        check(lib().nssb_bm3d_frame_window(self.handle, n, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def _frames(self, clip: Clip, first: int, last: int):
+        arr = (Frame * (last - first + 1))()
+        for i, n in enumerate(range(first, last + 1)):
+            for p, plane in enumerate(clip.frames[n]):
+                ptr, stride = _plane_ptr(plane)
+                arr[i].planes[p] = ptr
+                arr[i].strides[p] = stride
+        return arr
+
+    def get_frame(self, n: int, out=None):
+        """Output frame n: a tuple of planes (numpy, or torch CUDA tensors when the clip is device-resident)."""
+        first, last = self.frame_window(n)
+        device = self.clip.device
+        src = self._frames(self.clip, first, last)
+        ref = self._frames(self.ref, first, last) if self.ref is not None else None
+        if out is None:
+            shapes = [self.vi.plane_shape(p) for p in range(self.vi.planes())]
+            if device:
+                import torch
+
+                out = tuple(torch.empty(s, dtype=torch.float32, device=self.clip.frames[0][0].device) for s in shapes)
+            else:
+                out = tuple(np.empty(s, np.float32) for s in shapes)
+        fo = FrameOut()
+        for p, plane in enumerate(out):
+            ptr, stride = _plane_ptr(plane)
+            fo.planes[p] = ptr
+            fo.strides[p] = stride
+        check(lib().nssb_bm3d_get_frame(self.handle, n, src, ref, first, last - first + 1,
+                                        MEM_DEVICE if device else MEM_HOST, C.byref(fo)))
+        return out
+
+
+def BM3D(clip: Clip, ref: Clip | None = None, **kwargs) -> Node:
+    """core.nss_cuda.BM3D(clip, ref, ...) -- see docs/api/cuda/bm3d.md of the reference for the arguments."""
+    return Node(clip, ref, kwargs)
+
+
+def backend(device_id: int = 0) -> str:
+    buf = C.create_string_buffer(1024)
+    check(lib().nssb_backend_info(device_id, buf, len(buf)))
+    return buf.value.decode()
+
+
+def version() -> str:
+    return lib().nssb_version().decode()
+
+
+def build() -> None:
+    import subprocess
+
+    subprocess.run(["make", "-s", "-j8", "-C", str(HERE)], check=True)

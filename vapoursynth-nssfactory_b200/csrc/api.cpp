@@ -1,0 +1,202 @@
+// The C ABI (include/nss_b200.h): status codes and a per-thread error text,
+// no exception crosses it (the reference's checked_create / checked_frame
+// boundary, src/frontend/validate.hpp:36-52, src/frontend/ownership.hpp:157-165).
+#include "nss_b200.h"
+
+#include "engine.hpp"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+struct nssb_bm3d {
+    std::unique_ptr<nssb::Engine> engine;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& what) {
+    g_error = what;
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        g_error.clear();
+        f();
+        return NSSB_OK;
+    } catch (const nssb::ArgumentError& e) {
+        return fail(NSSB_ERR_ARGUMENT, e.what());
+    } catch (const nssb::CudaError& e) {
+        return fail(NSSB_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(NSSB_ERR_RESOURCE, "nss: resource allocation failed during creation");
+    } catch (const std::invalid_argument& e) {
+        return fail(NSSB_ERR_STATE, e.what());
+    } catch (const std::out_of_range& e) {
+        return fail(NSSB_ERR_STATE, e.what());
+    } catch (const std::exception& e) {
+        return fail(NSSB_ERR_STATE, e.what());
+    } catch (...) {
+        return fail(NSSB_ERR_STATE, "nss: unexpected failure");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nssb_last_error(void) { return g_error.c_str(); }
+
+const char* nssb_version(void) { return "nss_b200 1.0 (sm_100a)"; }
+
+int nssb_backend_info(int device_id, char* buf, size_t cap) {
+    return guarded([&] {
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        std::string s;
+        if (e != cudaSuccess || count == 0) {
+            (void)cudaGetLastError();
+            s = std::string("{\"device_count\": 0, \"error\": \"") + cudaGetErrorString(e) + "\"}";
+        } else {
+            if (device_id < 0 || device_id >= count) throw nssb::ArgumentError("nss_cuda.Backend: device_id out of range");
+            cudaDeviceProp prop{};
+            NSSB_CUDA(cudaGetDeviceProperties(&prop, device_id));
+            char tmp[512];
+            std::snprintf(tmp, sizeof tmp,
+                          "{\"device_count\": %d, \"device_id\": %d, \"name\": \"%s\", \"compute_capability\": "
+                          "\"%d.%d\", \"sm_count\": %d, \"memory_bytes\": %zu, \"kernels\": \"sm_100a\"}",
+                          count, device_id, prop.name, prop.major, prop.minor, prop.multiProcessorCount,
+                          (size_t)prop.totalGlobalMem);
+            s = tmp;
+        }
+        if (buf && cap) {
+            std::strncpy(buf, s.c_str(), cap - 1);
+            buf[cap - 1] = 0;
+        }
+    });
+}
+
+int nssb_bm3d_check(const nssb_video_info* clip, const nssb_video_info* ref, const nssb_arg* args, int nargs,
+                    nssb_video_info* out_vi) {
+    return guarded([&] {
+        if (!clip) throw nssb::ArgumentError("nss_cuda.BM3D: clip missing");
+        const nssb::Bm3dConfig cfg = nssb::parse_bm3d_call(*clip, ref, args, nargs);
+        if (out_vi) *out_vi = cfg.out_vi;
+    });
+}
+
+int nssb_bm3d_create(const nssb_video_info* clip, const nssb_video_info* ref, const nssb_arg* args, int nargs,
+                     nssb_bm3d** out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!clip || !out) throw nssb::ArgumentError("nss_cuda.BM3D: clip missing");
+        const nssb::Bm3dConfig cfg = nssb::parse_bm3d_call(*clip, ref, args, nargs);
+        // acquire_device (context.cpp:43-60): a creation error, never a render error
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0) {
+            (void)cudaGetLastError();
+            throw nssb::ArgumentError(std::string("nss_cuda.BM3D: no CUDA device available (") +
+                                      cudaGetErrorString(e) + ")");
+        }
+        if (cfg.device_id >= count)
+            throw nssb::ArgumentError("nss_cuda.BM3D: device_id " + std::to_string(cfg.device_id) +
+                                      " is out of range (" + std::to_string(count) + " devices)");
+        cudaDeviceProp prop{};
+        NSSB_CUDA(cudaGetDeviceProperties(&prop, cfg.device_id));
+        if (prop.major != 10 || prop.minor != 0)
+            throw nssb::ArgumentError("nss_cuda.BM3D: this build runs on sm_100 (B200) devices only");
+        auto h = std::make_unique<nssb_bm3d>();
+        h->engine = std::make_unique<nssb::Engine>(cfg);
+        *out = h.release();
+    });
+}
+
+void nssb_bm3d_free(nssb_bm3d* h) { delete h; }
+
+int nssb_bm3d_output_info(const nssb_bm3d* h, nssb_video_info* out_vi) {
+    return guarded([&] {
+        if (!h || !out_vi) throw std::invalid_argument("nss_cuda.BM3D: null handle");
+        *out_vi = h->engine->config().out_vi;
+    });
+}
+
+int nssb_bm3d_frame_window(const nssb_bm3d* h, int n, int* first, int* last) {
+    return guarded([&] {
+        if (!h || !first || !last) throw std::invalid_argument("nss_cuda.BM3D: null handle");
+        h->engine->frame_window(n, first, last);
+    });
+}
+
+int nssb_bm3d_get_frame(nssb_bm3d* h, int n, const nssb_frame* clip_frames, const nssb_frame* ref_frames, int first,
+                        int count, int memory, nssb_frame_out* out) {
+    return guarded([&] {
+        if (!h || !clip_frames || !out) throw std::invalid_argument("nss_cuda.BM3D: null argument");
+        if (memory != NSSB_MEM_HOST && memory != NSSB_MEM_DEVICE)
+            throw std::invalid_argument("nss_cuda.BM3D: memory must be NSSB_MEM_HOST or NSSB_MEM_DEVICE");
+        h->engine->get_frame(n, clip_frames, ref_frames, first, count, memory, out);
+    });
+}
+
+int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stats* out) {
+    return guarded([&] {
+        if (!h) throw std::invalid_argument("nss_cuda.BM3D: null handle");
+        h->engine->stats(enable_timing, reset, out);
+    });
+}
+
+int nssb_match_spatial(const float* plane, int64_t stride, int width, int height, int block, int step,
+                       int bm_range, int group, int32_t* pos, float* dist, int32_t* count, void* stream) {
+    return guarded([&] {
+        if (!plane || !pos || !count || width < block || height < block || block < 1 || step < 1 || group < 1 ||
+            group > nssb::kMaxGroup || bm_range < 0 || bm_range > nssb::kMaxRange || width > 65535 || height > 65535)
+            throw std::invalid_argument("nss_cuda: invalid matching arguments");
+        nssb::launch_match_spatial(plane, stride, width, height, block, step, bm_range, group, pos, dist, count,
+                                   static_cast<cudaStream_t>(stream));
+    });
+}
+
+int nssb_match_temporal(const float* const* planes, const int64_t* strides, int ntemp, int t0, int valid_begin,
+                        int valid_end, int width, int height, int block, int step, int bm_range, int group,
+                        int ps_num, int ps_range, int32_t* pos, int32_t* slot, float* dist, int32_t* count,
+                        void* stream) {
+    return guarded([&] {
+        if (!planes || !strides || !pos || !slot || !dist || !count || ntemp < 1 || ntemp > nssb::kMaxSlots ||
+            t0 < 0 || t0 >= ntemp || width < block || height < block || group < 1 || group > nssb::kMaxGroup ||
+            ps_num < 1 || ps_num > group || ps_range < 0)
+            throw std::invalid_argument("nss_cuda: invalid temporal matching arguments");
+        nssb::TemporalPlanes tp{};
+        for (int t = 0; t < ntemp; ++t) {
+            tp.plane[t] = planes[t];
+            tp.stride[t] = strides[t];
+        }
+        auto s = static_cast<cudaStream_t>(stream);
+        nssb::launch_match_spatial(planes[t0], strides[t0], width, height, block, step, bm_range, group, pos, dist,
+                                   count, s);
+        nssb::launch_match_temporal(tp, ntemp, t0, valid_begin, valid_end, width, height, block, step, group, ps_num,
+                                    ps_range, pos, slot, dist, count, s);
+    });
+}
+
+int nssb_bm3d_plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int width, int height,
+                          float sigma, int block, int group, int step, int bm_range, void* stream) {
+    return guarded([&] {
+        if (!src || !dst || width < block || height < block || block < 1 || step < 1 || step > block ||
+            group < 1 || group > nssb::kMaxGroup || bm_range < 0 || bm_range > nssb::kMaxRange)
+            throw std::invalid_argument("nss_cuda: invalid stage arguments");
+        nssb::StageParams sp;
+        sp.sigma = sigma;
+        sp.block = block;
+        sp.group = group;
+        sp.step = step;
+        sp.bm_range = bm_range;
+        nssb::Engine::plane_stage(src, ref, dst, stride, width, height, sp, static_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Shared device/host helpers of the sm_100a BM3D library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace nssb {
+
+// A failed CUDA call; the C ABI turns it into NSSB_ERR_CUDA with this text
+// (the reference's CudaError, src/cuda/runtime/error.hpp:14-47).
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        throw CudaError(std::string("nss_cuda: ") + what + " failed: " + cudaGetErrorString(e) + " (" + file + ":" +
+                        std::to_string(line) + ")");
+    }
+}
+#define NSSB_CUDA(call) ::nssb::cuda_check((call), #call, __FILE__, __LINE__)
+
+// Fixed-point scale of the aggregation sums: num and the per-origin weights
+// are int64 multiples of 2^-32, so the sums do not depend on the order in
+// which groups land (deterministic in any launch shape or batch mix).
+constexpr double kFixedScale = 4294967296.0;
+constexpr double kFixedInv = 1.0 / 4294967296.0;
+
+__host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ inline int grid_count(int extent, int block, int step) {
+    return extent < block ? 0 : (extent - block + step - 1) / step + 1;
+}
+__host__ __device__ inline int grid_pos(int i, int extent, int block, int step) {
+    const int p = i * step;
+    return p < extent - block ? p : extent - block;
+}
+
+// Packed match position: y in the high half, x in the low half.
+__host__ __device__ inline int32_t pack_pos(int x, int y) { return static_cast<int32_t>((uint32_t(y) << 16) | uint32_t(x)); }
+__host__ __device__ inline int pos_x(int32_t p) { return static_cast<int>(uint32_t(p) & 0xffffu); }
+__host__ __device__ inline int pos_y(int32_t p) { return static_cast<int>(uint32_t(p) >> 16); }
+
+}  // namespace nssb

@@ -1,0 +1,407 @@
+// Host engine (see engine.hpp). Radius-0 frames run the stages per plane on
+// device-resident copies; the temporal drivers live in temporal_engine.cu.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace nssb {
+
+void* dev_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) return nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    return p;
+}
+
+void dev_free(void* p) {
+    if (p) (void)cudaFree(p);
+}
+
+namespace {
+
+int64_t pitch_of(int w) { return (int64_t)((w + 31) / 32) * 32; }
+
+}  // namespace
+
+Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg) {
+    device_ = cfg.device_id;
+    NSSB_CUDA(cudaSetDevice(device_));
+    NSSB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    try {
+        alloc();
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+Engine::~Engine() { release(); }
+
+void Engine::release() {
+    for (auto& e : event_pool_) {
+        (void)cudaEventDestroy(e.first);
+        (void)cudaEventDestroy(e.second);
+    }
+    event_pool_.clear();
+    for (void* p : allocations_) dev_free(p);
+    allocations_.clear();
+    if (stream_) {
+        (void)cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+    }
+}
+
+struct Engine::Plan {};
+
+void Engine::alloc() {
+    auto take = [&](size_t bytes) {
+        void* p = dev_alloc(bytes);
+        allocations_.push_back(p);
+        return p;
+    };
+    for (int p = 0; p < cfg_.planes; ++p) {
+        const int w = cfg_.plane_w[p], h = cfg_.plane_h[p];
+        const int64_t pitch = pitch_of(w);
+        for (DevPlane* d : {&in_[p], &refin_[p], &basic_[p], &out_[p]}) {
+            d->p = static_cast<float*>(take((size_t)pitch * h * sizeof(float)));
+            d->pitch = pitch;
+            d->w = w;
+            d->h = h;
+        }
+        // num stays zero between stages: every finish clears what it consumed
+        acc_[p].pitch = pitch;
+        acc_[p].num = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
+        acc_[p].wsum = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
+        NSSB_CUDA(cudaMemset(acc_[p].num, 0, (size_t)pitch * h * sizeof(long long)));
+        size_t jobs = 0, group = 0, cube = 0;
+        for (const StageParams* sp : {&cfg_.final_stage[p], &cfg_.basic_stage[p]}) {
+            jobs = std::max(jobs, (size_t)grid_count(w, sp->block, sp->step) * grid_count(h, sp->block, sp->step));
+            group = std::max(group, (size_t)sp->group);
+            cube = std::max(cube, group_filter_scratch_floats(sp->block, sp->group, true));
+        }
+        StageScratch& sc = scratch_[p];
+        sc.jobs_cap = jobs;
+        sc.group_cap = group;
+        sc.pos = static_cast<int32_t*>(take(jobs * group * sizeof(int32_t)));
+        sc.slot = static_cast<int32_t*>(take(jobs * group * sizeof(int32_t)));
+        sc.dist = static_cast<float*>(take(jobs * group * sizeof(float)));
+        sc.count = static_cast<int32_t*>(take(jobs * sizeof(int32_t)));
+        sc.cube_floats = cube;
+        if (cube) sc.cube = static_cast<float*>(take(cube * sizeof(float)));
+    }
+}
+
+void Engine::frame_window(int n, int* first, int* last) const {
+    // The arInitial requests of getFrame: a rolling stage needs the windows of
+    // the centres n-r..n+r, final=1 those of the basic frames behind them.
+    const int r = cfg_.radius;
+    const int reach = r == 0 ? 0 : cfg_.rolling ? (cfg_.two_stage ? 4 * r : 2 * r) : (cfg_.two_stage ? 3 * r : r);
+    *first = std::max(0, n - reach);
+    *last = std::min(cfg_.vi.num_frames - 1, n + reach);
+}
+
+const float* Engine::device_input(int plane, const nssb_frame* frames, int first, int n, int memory, bool is_ref,
+                                  int64_t* stride) {
+    const nssb_frame& f = frames[n - first];
+    if (memory == NSSB_MEM_DEVICE) {
+        *stride = f.strides[plane];
+        return f.planes[plane];
+    }
+    DevPlane& d = is_ref ? refin_[plane] : in_[plane];
+    NSSB_CUDA(cudaMemcpy2DAsync(d.p, d.pitch * sizeof(float), f.planes[plane], f.strides[plane] * sizeof(float),
+                                d.w * sizeof(float), d.h, cudaMemcpyHostToDevice, stream_));
+    *stride = d.pitch;
+    return d.p;
+}
+
+template <class F>
+void Engine::timed(Kind kind, F&& launch) {
+    if (!timing_) {
+        launch();
+    } else {
+        const size_t i = pending_.size();
+        if (i >= event_pool_.size()) {
+            cudaEvent_t a, b;
+            NSSB_CUDA(cudaEventCreate(&a));
+            NSSB_CUDA(cudaEventCreate(&b));
+            event_pool_.emplace_back(a, b);
+        }
+        NSSB_CUDA(cudaEventRecord(event_pool_[i].first, stream_));
+        launch();
+        NSSB_CUDA(cudaEventRecord(event_pool_[i].second, stream_));
+        pending_.emplace_back((int)kind, i);
+    }
+    ++stats_.launches;
+    if (kind == kMatch) ++stats_.match_launches;
+    if (kind == kGroup) ++stats_.group_launches;
+    if (kind == kFinish) ++stats_.finish_launches;
+}
+
+// After the stream is synchronised: add the bracketed durations.
+void Engine::collect_timing() {
+    for (const auto& p : pending_) {
+        float ms = 0.f;
+        NSSB_CUDA(cudaEventElapsedTime(&ms, event_pool_[p.second].first, event_pool_[p.second].second));
+        if (p.first == kMatch) stats_.match_ms += ms;
+        if (p.first == kGroup) stats_.group_ms += ms;
+        if (p.first == kFinish) stats_.finish_ms += ms;
+    }
+    pending_.clear();
+}
+
+// Algorithmic work of one matching launch: every reference against every
+// other position of its clamped window, 3 * B^2 flops per pair.
+void Engine::count_match(int w, int h, const StageParams& sp) {
+    auto axis = [&](int extent) {
+        const int n = grid_count(extent, sp.block, sp.step);
+        double sum = 0;
+        for (int i = 0; i < n; ++i) {
+            const int c = grid_pos(i, extent, sp.block, sp.step);
+            sum += std::min(c + sp.bm_range, extent - sp.block) - std::max(c - sp.bm_range, 0) + 1;
+        }
+        return std::make_pair(sum, (double)n);
+    };
+    const auto ax = axis(w), ay = axis(h);
+    const double pairs = ax.first * ay.first - ax.second * ay.second;
+    stats_.match_pairs += pairs;
+    stats_.match_flops += pairs * 3.0 * sp.block * sp.block;
+}
+
+void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (out) *out = stats_;
+    if (reset) stats_ = nssb_kernel_stats{};
+    timing_ = enable_timing != 0;
+}
+
+// One stage over several planes (radius 0): match on ref (Wiener) or src
+// (hard threshold), filter every group, finish. Planes that share a shape go
+// through one launch per kernel; sigma 0 copies the plane.
+void Engine::run_stage(StageItem* items, int n) {
+    int live[3], nl = 0;
+    for (int i = 0; i < n; ++i) {
+        const StageItem& it = items[i];
+        const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
+        if (it.sp->sigma == 0.f) {
+            NSSB_CUDA(cudaMemcpy2DAsync(it.dst, it.dstride * sizeof(float), it.src, it.sstride * sizeof(float),
+                                        w * sizeof(float), h, cudaMemcpyDeviceToDevice, stream_));
+        } else {
+            live[nl++] = i;
+        }
+    }
+    bool done[3] = {false, false, false};
+    for (int a = 0; a < nl; ++a) {
+        if (done[a]) continue;
+        // the planes of this shape
+        int set[3], ns = 0;
+        const StageItem& first = items[live[a]];
+        for (int b = a; b < nl; ++b) {
+            const StageItem& it = items[live[b]];
+            const StageParams &x = *it.sp, &y = *first.sp;
+            if (!done[b] && x.block == y.block && x.group == y.group && x.step == y.step && x.bm_range == y.bm_range &&
+                (it.ref != nullptr) == (first.ref != nullptr)) {
+                set[ns++] = live[b];
+                done[b] = true;
+            }
+        }
+        const StageParams& sp = *first.sp;
+        const bool wiener = first.ref != nullptr;
+        // matching: batched 8x8 kernel when the shape has it, else the generic one per plane
+        mbatch_.n = 0;
+        mbatch_.step = sp.step;
+        for (int q = 0; q < ns; ++q) {
+            const StageItem& it = items[set[q]];
+            if (it.shared_pos) continue;
+            StageScratch& sc = scratch_[it.plane];
+            mbatch_.p[mbatch_.n++] = MatchPlane{wiener ? it.ref : it.src, wiener ? it.rstride : it.sstride, sc.pos,
+                                                sc.dist, sc.count, cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], 0,
+                                                0, 0};
+            count_match(cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], sp);
+        }
+        if (mbatch_.n > 0) {
+            bool ok = false;
+            if (sp.block == 8) timed(kMatch, [&] { ok = launch_match8_batch(mbatch_, sp.bm_range, sp.group, stream_); });
+            if (!ok) {
+                for (int q = 0; q < mbatch_.n; ++q) {
+                    const MatchPlane& m = mbatch_.p[q];
+                    timed(kMatch, [&] {
+                        launch_match_spatial(m.src, m.stride, m.W, m.H, sp.block, sp.step, sp.bm_range, sp.group,
+                                             m.pos, m.dist, m.count, stream_);
+                    });
+                }
+            }
+        }
+        for (int q = 0; q < ns; ++q) {
+            const AccPlane& ac = acc_[items[set[q]].plane];
+            NSSB_CUDA(cudaMemsetAsync(ac.wsum, 0, (size_t)ac.pitch * cfg_.plane_h[items[set[q]].plane] * 8, stream_));
+        }
+        // group filtering
+        gbatch_.n = 0;
+        gbatch_.total_jobs = 0;
+        for (int q = 0; q < ns; ++q) {
+            const StageItem& it = items[set[q]];
+            const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
+            const int jobs = grid_count(w, sp.block, sp.step) * grid_count(h, sp.block, sp.step);
+            const AccPlane& ac = acc_[it.plane];
+            const StageScratch& sc = scratch_[it.plane];
+            gbatch_.p[gbatch_.n++] = GroupPlane{it.src, it.ref, it.sstride, it.rstride, ac.num, ac.wsum, ac.pitch,
+                                                it.shared_pos ? it.shared_pos : sc.pos,
+                                                it.shared_count ? it.shared_count : sc.count, gbatch_.total_jobs, jobs,
+                                                it.sp->sigma};
+            gbatch_.total_jobs += jobs;
+        }
+        bool gok = false;
+        if (sp.block == 8) timed(kGroup, [&] { gok = launch_group8_batch(gbatch_, sp.group, wiener, stream_); });
+        if (!gok) {
+            for (int q = 0; q < gbatch_.n; ++q) {
+                const GroupPlane& g = gbatch_.p[q];
+                const StageItem& it = items[set[q]];
+                GroupIO io{};
+                io.src[0] = g.src;
+                io.ref[0] = g.ref;
+                io.stride = g.stride;
+                io.ref_stride = g.ref_stride;
+                io.num[0] = g.num;
+                io.wsum[0] = g.wsum;
+                io.acc_stride = g.acc_stride;
+                const StageScratch& sc = scratch_[it.plane];
+                timed(kGroup, [&] {
+                    launch_group_filter(io, cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], g.pos, nullptr, g.count,
+                                        g.njobs, sp.block, sp.group, g.sigma, wiener, sc.cube, sc.cube_floats,
+                                        stream_);
+                });
+            }
+        }
+        // finish (clears num)
+        fbatch_.n = 0;
+        fbatch_.block = sp.block;
+        fbatch_.total_ctas = 0;
+        for (int q = 0; q < ns; ++q) {
+            const StageItem& it = items[set[q]];
+            const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
+            const AccPlane& ac = acc_[it.plane];
+            fbatch_.p[fbatch_.n++] = FinishPlane{ac.num, ac.wsum, ac.pitch, it.src, it.sstride, it.dst, it.dstride, w,
+                                                 h, finish_tiles_x(w), fbatch_.total_ctas};
+            fbatch_.total_ctas += finish_tiles(w, h);
+        }
+        timed(kFinish, [&] { launch_finish_batch(fbatch_, stream_); });
+    }
+}
+
+void Engine::spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory) {
+    const float* src[3]{};
+    const float* rp[3]{};
+    int64_t ss[3]{}, rs[3]{};
+    for (int p = 0; p < cfg_.planes; ++p) {
+        src[p] = device_input(p, clip, first, n, memory, false, &ss[p]);
+        if (cfg_.has_ref) rp[p] = device_input(p, ref, first, n, memory, true, &rs[p]);
+    }
+    StageItem items[3];
+    const int np = cfg_.planes;
+    // CBM3D (filter_bm3d.cpp:451-486): plane 0's groups serve every plane; a
+    // plane-0 sigma of 0 still matches (on plane 0) for the others.
+    auto chroma_link = [&](const StageParams* sps, bool wiener) {
+        if (!cfg_.chroma) return;
+        if (sps[0].sigma == 0.f) {
+            const StageParams& s0 = sps[0];
+            const int w = cfg_.plane_w[0], h = cfg_.plane_h[0];
+            StageScratch& sc = scratch_[0];
+            timed(kMatch, [&] {
+                launch_match_spatial(wiener ? items[0].ref : items[0].src, wiener ? items[0].rstride : items[0].sstride,
+                                     w, h, s0.block, s0.step, s0.bm_range, s0.group, sc.pos, sc.dist, sc.count,
+                                     stream_);
+            });
+        }
+        for (int p = 1; p < np; ++p) {
+            items[p].shared_pos = scratch_[0].pos;
+            items[p].shared_count = scratch_[0].count;
+        }
+    };
+    if (cfg_.two_stage) {
+        for (int p = 0; p < np; ++p)
+            items[p] = StageItem{p, &cfg_.basic_stage[p], src[p], ss[p], nullptr, 0, basic_[p].p, basic_[p].pitch};
+        chroma_link(cfg_.basic_stage, false);
+        run_stage(items, np);
+        for (int p = 0; p < np; ++p)
+            items[p] = StageItem{p, &cfg_.final_stage[p], src[p], ss[p], basic_[p].p, basic_[p].pitch, out_[p].p,
+                                 out_[p].pitch};
+        chroma_link(cfg_.final_stage, true);
+        run_stage(items, np);
+    } else {
+        for (int p = 0; p < np; ++p)
+            items[p] = StageItem{p, &cfg_.final_stage[p], src[p], ss[p], cfg_.has_ref ? rp[p] : nullptr, rs[p],
+                                 out_[p].p, out_[p].pitch};
+        chroma_link(cfg_.final_stage, cfg_.has_ref);
+        run_stage(items, np);
+    }
+}
+
+void Engine::get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
+                       nssb_frame_out* out) {
+    std::lock_guard<std::mutex> lock(mu_);
+    NSSB_CUDA(cudaSetDevice(device_));
+    if (n < 0 || n >= cfg_.vi.num_frames) throw std::out_of_range("nss_cuda.BM3D: frame number out of range");
+    int wf = 0, wl = 0;
+    frame_window(n, &wf, &wl);
+    if (first > wf || first + count - 1 < wl) throw std::out_of_range("nss_cuda.BM3D: input frames do not cover the window");
+    if (cfg_.has_ref && !ref) throw std::invalid_argument("nss_cuda.BM3D: ref frames missing");
+    if (cfg_.radius > 0) {
+        temporal_frame(n, clip, ref, first, count, memory, out);
+        return;
+    }
+    spatial_frame(n, clip, ref, first, memory);
+    for (int p = 0; p < cfg_.planes; ++p) {
+        const DevPlane& o = out_[p];
+        NSSB_CUDA(cudaMemcpy2DAsync(out->planes[p], out->strides[p] * sizeof(float), o.p, o.pitch * sizeof(float),
+                                    o.w * sizeof(float), o.h,
+                                    memory == NSSB_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    stream_));
+    }
+    NSSB_CUDA(cudaStreamSynchronize(stream_));
+    collect_timing();
+}
+
+void Engine::plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,
+                         const StageParams& sp, cudaStream_t stream) {
+    if (sp.sigma == 0.f) {
+        NSSB_CUDA(cudaMemcpy2DAsync(dst, stride * 4, src, stride * 4, w * 4, h, cudaMemcpyDeviceToDevice, stream));
+        return;
+    }
+    const size_t jobs = (size_t)grid_count(w, sp.block, sp.step) * grid_count(h, sp.block, sp.step);
+    const size_t cube = group_filter_scratch_floats(sp.block, sp.group, ref != nullptr);
+    int32_t *pos = nullptr, *count = nullptr;
+    float* dist = nullptr;
+    long long *num = nullptr, *wsum = nullptr;
+    float* cubes = nullptr;
+    const size_t plane = (size_t)stride * h;
+    NSSB_CUDA(cudaMallocAsync(&pos, jobs * sp.group * 4, stream));
+    NSSB_CUDA(cudaMallocAsync(&dist, jobs * sp.group * 4, stream));
+    NSSB_CUDA(cudaMallocAsync(&count, jobs * 4, stream));
+    NSSB_CUDA(cudaMallocAsync(&num, plane * 8, stream));
+    NSSB_CUDA(cudaMallocAsync(&wsum, plane * 8, stream));
+    if (cube) NSSB_CUDA(cudaMallocAsync(&cubes, cube * 4, stream));
+    launch_match_spatial(ref ? ref : src, stride, w, h, sp.block, sp.step, sp.bm_range, sp.group, pos, dist, count,
+                         stream);
+    NSSB_CUDA(cudaMemsetAsync(num, 0, plane * 8, stream));
+    NSSB_CUDA(cudaMemsetAsync(wsum, 0, plane * 8, stream));
+    GroupIO io{};
+    io.src[0] = src;
+    io.ref[0] = ref;
+    io.stride = stride;
+    io.ref_stride = stride;
+    io.num[0] = num;
+    io.wsum[0] = wsum;
+    io.acc_stride = stride;
+    launch_group_filter(io, w, h, pos, nullptr, count, (int)jobs, sp.block, sp.group, sp.sigma, ref != nullptr, cubes,
+                        cube, stream);
+    launch_finish(num, wsum, stride, src, stride, dst, stride, w, h, sp.block, stream);
+    for (void* p : {(void*)pos, (void*)dist, (void*)count, (void*)num, (void*)wsum, (void*)cubes})
+        if (p) NSSB_CUDA(cudaFreeAsync(p, stream));
+}
+
+}  // namespace nssb

@@ -1,0 +1,126 @@
+// Host engine of one BM3D filter instance: device buffers, the stage pipeline
+// (match -> group filter -> finish) and the frame-level drivers (spatial,
+// two-stage, CBM3D, rolling temporal and the legacy intermediate).
+// Reference counterparts: the group driver src/cuda/common/group_driver.{hpp,cpp}
+// (memory plan :571-600, filter_center :760-856, first stage :877-898, frame
+// path :968-1107, rolling :1207-1800).
+#pragma once
+
+#include "kernels.cuh"
+#include "params.hpp"
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace nssb {
+
+// A pitched device plane owned by the engine.
+struct DevPlane {
+    float* p = nullptr;
+    int64_t pitch = 0;  // elements
+    int w = 0, h = 0;
+};
+
+// Fixed-point accumulators of one target frame plane.
+struct AccPlane {
+    long long* num = nullptr;
+    long long* wsum = nullptr;
+    int64_t pitch = 0;
+};
+
+// Scratch of one stage pass: match lists, group cubes.
+struct StageScratch {
+    int32_t* pos = nullptr;
+    int32_t* slot = nullptr;
+    float* dist = nullptr;
+    int32_t* count = nullptr;
+    size_t jobs_cap = 0, group_cap = 0;
+    float* cube = nullptr;
+    size_t cube_floats = 0;
+};
+
+// One plane of one stage of a frame: where it reads, matches and writes.
+struct StageItem {
+    int plane;                 // engine plane (scratch and accumulators)
+    const StageParams* sp;
+    const float* src;          // filtered plane
+    int64_t sstride;
+    const float* ref;          // Wiener reference and match source, or null (hard threshold)
+    int64_t rstride;
+    float* dst;
+    int64_t dstride;
+    const int32_t* shared_pos = nullptr;  // CBM3D: groups matched on another plane
+    const int32_t* shared_count = nullptr;
+};
+
+// Plane pointers of one stage invocation on the device.
+struct StagePlanes {
+    const float* src[kMaxSlots]{};    // filtered planes per slot
+    int64_t src_stride = 0;
+    const float* ref[kMaxSlots]{};    // Wiener reference per slot (also the match source), or null
+    int64_t ref_stride = 0;
+};
+
+class Engine {
+public:
+    explicit Engine(const Bm3dConfig& cfg);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    const Bm3dConfig& config() const { return cfg_; }
+    void frame_window(int n, int* first, int* last) const;
+    void get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
+                   nssb_frame_out* out);
+
+    // Kernel accounting (nssb_bm3d_stats).
+    void stats(int enable_timing, int reset, nssb_kernel_stats* out);
+
+    // One radius-0 stage of one plane on caller device memory (the C ABI's
+    // nssb_bm3d_plane_stage).
+    static void plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,
+                            const StageParams& sp, cudaStream_t stream);
+
+private:
+    struct Plan;
+    void alloc();
+    void release();
+    const float* device_input(int plane, const nssb_frame* frames, int first, int n, int memory, bool is_ref,
+                              int64_t* stride);
+    void spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory);
+    // Runs one stage over several planes: one launch per kernel and shape.
+    void run_stage(StageItem* items, int n);
+    void temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
+                        nssb_frame_out* out);
+
+    enum Kind { kMatch = 0, kGroup = 1, kFinish = 2 };
+    template <class F>
+    void timed(Kind kind, F&& launch);
+    void collect_timing();
+    void count_match(int w, int h, const StageParams& sp);
+
+    Bm3dConfig cfg_;
+    int device_ = 0;
+    bool timing_ = false;
+    nssb_kernel_stats stats_{};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool_;
+    std::vector<std::pair<int, size_t>> pending_;  // (kind, event pair index)
+    cudaStream_t stream_ = nullptr;
+    std::mutex mu_;
+    DevPlane in_[3], refin_[3], basic_[3], out_[3];
+    AccPlane acc_[3];
+    StageScratch scratch_[3];
+    MatchBatch mbatch_;
+    GroupBatch gbatch_;
+    FinishBatch fbatch_;
+    std::vector<void*> allocations_;
+    std::unique_ptr<Plan> plan_;
+};
+
+// Device memory helpers (cudaMalloc'd, recorded for release).
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+
+}  // namespace nssb

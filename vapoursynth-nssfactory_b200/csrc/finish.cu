@@ -1,0 +1,137 @@
+// Finish of a stage (sm_100a): den is recovered exactly from the per-origin
+// weights by a B x B box sum in int64, then out = den > 1e-12 ? num / den : src
+// (reference aggregate_finish, src/cpu/bm/agg.cpp:17-42; the device form keeps
+// den at the patch origin too, src/cuda/common/aggregate.cu:300-323).
+#include "kernels.cuh"
+
+namespace nssb {
+namespace {
+
+constexpr int kTX = 32, kTY = 8, kMaxB = 32;
+
+// Box-summed den of the tile's pixels into den_tile[kTY][kTX] (int64).
+__device__ void box_den(const long long* __restrict__ wsum, int64_t as, int W, int H, int B, int x0, int y0,
+                        long long (*wt)[kTX + kMaxB - 1], long long (*hs)[kTX], long long (*den)[kTX]) {
+    const int rows = kTY + B - 1, cols = kTX + B - 1;
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        const int r = i / cols, c = i - r * cols;
+        const int yy = y0 - B + 1 + r, xx = x0 - B + 1 + c;
+        wt[r][c] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? wsum[(int64_t)yy * as + xx] : 0ll;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * kTX; i += blockDim.x) {
+        const int r = i / kTX, c = i - r * kTX;
+        long long s = 0;
+        for (int q = 0; q < B; ++q) s += wt[r][c + q];
+        hs[r][c] = s;
+    }
+    __syncthreads();
+    {
+        const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
+        long long s = 0;
+        for (int q = 0; q < B; ++q) s += hs[r + q][c];
+        den[r][c] = s;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kTX* kTY) finish_kernel(const long long* __restrict__ num,
+                                                          const long long* __restrict__ wsum, int64_t as,
+                                                          const float* __restrict__ src, int64_t ss,
+                                                          float* __restrict__ dst, int64_t ds, int W, int H, int B) {
+    __shared__ long long wt[kTY + kMaxB - 1][kTX + kMaxB - 1];
+    __shared__ long long hs[kTY + kMaxB - 1][kTX];
+    __shared__ long long den[kTY][kTX];
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+    box_den(wsum, as, W, H, B, x0, y0, wt, hs, den);
+    const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
+    const int x = x0 + c, y = y0 + r;
+    if (x >= W || y >= H) return;
+    const long long d = den[r][c];
+    const double dd = (double)d * kFixedInv;
+    float out;
+    if ((float)dd > 1e-12f) {
+        out = (float)((double)num[(int64_t)y * as + x] / (double)d);
+    } else {
+        out = src[(int64_t)y * ss + x];
+    }
+    dst[(int64_t)y * ds + x] = out;
+}
+
+__global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restrict__ num,
+                                                       const long long* __restrict__ wsum, int64_t as,
+                                                       float* __restrict__ dnum, float* __restrict__ dden,
+                                                       int64_t ds, int W, int H, int B) {
+    __shared__ long long wt[kTY + kMaxB - 1][kTX + kMaxB - 1];
+    __shared__ long long hs[kTY + kMaxB - 1][kTX];
+    __shared__ long long den[kTY][kTX];
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+    box_den(wsum, as, W, H, B, x0, y0, wt, hs, den);
+    const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
+    const int x = x0 + c, y = y0 + r;
+    if (x >= W || y >= H) return;
+    dnum[(int64_t)y * ds + x] = (float)((double)num[(int64_t)y * as + x] * kFixedInv);
+    dden[(int64_t)y * ds + x] = (float)((double)den[r][c] * kFixedInv);
+}
+
+// Batched finish over a plane table; num is cleared as it is consumed (each
+// pixel's num is read by exactly one thread), so the next stage finds it zero.
+__global__ void __launch_bounds__(kTX* kTY) finish_batch_kernel(const __grid_constant__ FinishBatch fb) {
+    __shared__ long long wt[kTY + kMaxB - 1][kTX + kMaxB - 1];
+    __shared__ long long hs[kTY + kMaxB - 1][kTX];
+    __shared__ long long den[kTY][kTX];
+    int pl = 0;
+    {
+        int lo = 0, hi = fb.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (fb.p[mid].cta0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        }
+        pl = lo;
+    }
+    const FinishPlane& P = fb.p[pl];
+    const int local = blockIdx.x - P.cta0;
+    const int ty = local / P.tiles_x, tx = local - ty * P.tiles_x;
+    const int x0 = tx * kTX, y0 = ty * kTY;
+    box_den(P.wsum, P.acc_stride, P.W, P.H, fb.block, x0, y0, wt, hs, den);
+    const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
+    const int x = x0 + c, y = y0 + r;
+    if (x >= P.W || y >= P.H) return;
+    const long long d = den[r][c];
+    long long* np = P.num + (int64_t)y * P.acc_stride + x;
+    const long long nv = *np;
+    *np = 0;
+    const double dd = (double)d * kFixedInv;
+    P.dst[(int64_t)y * P.dstride + x] = (float)dd > 1e-12f ? (float)((double)nv / (double)d)
+                                                           : P.src[(int64_t)y * P.sstride + x];
+}
+
+}  // namespace
+
+void launch_finish_batch(const FinishBatch& fb, cudaStream_t stream) {
+    if (fb.total_ctas <= 0) return;
+    finish_batch_kernel<<<fb.total_ctas, kTX * kTY, 0, stream>>>(fb);
+    NSSB_CUDA(cudaGetLastError());
+}
+
+int finish_tiles_x(int w) { return ceil_div(w, kTX); }
+int finish_tiles(int w, int h) { return ceil_div(w, kTX) * ceil_div(h, kTY); }
+
+void launch_finish(const long long* num, const long long* wsum, int64_t acc_stride, const float* src,
+                   int64_t sstride, float* dst, int64_t dstride, int width, int height, int block,
+                   cudaStream_t stream) {
+    const dim3 grid(ceil_div(width, kTX), ceil_div(height, kTY));
+    finish_kernel<<<grid, kTX * kTY, 0, stream>>>(num, wsum, acc_stride, src, sstride, dst, dstride, width, height,
+                                                  block);
+    NSSB_CUDA(cudaGetLastError());
+}
+
+void launch_fat_slice(const long long* num, const long long* wsum, int64_t acc_stride, float* dst_num,
+                      float* dst_den, int64_t dstride, int width, int height, int block, cudaStream_t stream) {
+    const dim3 grid(ceil_div(width, kTX), ceil_div(height, kTY));
+    fat_kernel<<<grid, kTX * kTY, 0, stream>>>(num, wsum, acc_stride, dst_num, dst_den, dstride, width, height,
+                                               block);
+    NSSB_CUDA(cudaGetLastError());
+}
+
+}  // namespace nssb

@@ -1,0 +1,356 @@
+// Collaborative filtering for 8x8 blocks and groups of 4, 8 or 16 (sm_100a):
+// the default BM3D shapes. Same semantics as group.cu (the reference's
+// Bm3dFilterGroup, src/cpu/bm/dct8.cpp:926-1133); the schedule is one warp
+// per group, the cube in registers and a padded per-warp shared buffer:
+//   - 32/G lanes per patch, each holding 8G/32 rows, then as many columns,
+//     then two Haar tubes (coefficient positions l and l+32 across the group);
+//   - the per-patch stride is 64 + 32/G floats, so the column and tube
+//     phases of the 32 lanes touch 32 different banks;
+//   - the 8-point DCT-II is evaluated through its even/odd symmetry: with
+//     a_n = x_n + x_{7-n}, b_n = x_n - x_{7-n}, the even outputs are a 4-point
+//     DCT of a (split again the same way) and the odd outputs a 4x4 cosine
+//     product with b, 36 operations instead of 64 multiply-adds; the inverse
+//     is the transpose of the same factorisation.
+#include "kernels.cuh"
+
+#include <cmath>
+
+namespace nssb {
+namespace {
+
+// cos(pi * m / 16) for m = 1..7
+constexpr float kC1 = 0.98078528040323044913f, kC2 = 0.92387953251128675613f, kC3 = 0.83146961230254523708f;
+constexpr float kC5 = 0.55557023301960222474f, kC6 = 0.38268343236508977173f, kC7 = 0.19509032201612826785f;
+constexpr float kS8 = 0.35355339059327376220f;  // 1/sqrt(8)
+
+__device__ __forceinline__ void fdct8(float* x) {
+    const float a0 = x[0] + x[7], a1 = x[1] + x[6], a2 = x[2] + x[5], a3 = x[3] + x[4];
+    const float b0 = x[0] - x[7], b1 = x[1] - x[6], b2 = x[2] - x[5], b3 = x[3] - x[4];
+    const float e0 = a0 + a3, e1 = a1 + a2, o0 = a0 - a3, o1 = a1 - a2;
+    x[0] = (e0 + e1) * kS8;
+    x[4] = (e0 - e1) * kS8;
+    x[2] = fmaf(0.5f * kC2, o0, 0.5f * kC6 * o1);
+    x[6] = fmaf(0.5f * kC6, o0, -0.5f * kC2 * o1);
+    // odd: X_k = 1/2 sum_n cos(pi (2n+1) k / 16) b_n
+    x[1] = 0.5f * fmaf(kC1, b0, fmaf(kC3, b1, fmaf(kC5, b2, kC7 * b3)));
+    x[3] = 0.5f * fmaf(kC3, b0, fmaf(-kC7, b1, fmaf(-kC1, b2, -kC5 * b3)));
+    x[5] = 0.5f * fmaf(kC5, b0, fmaf(-kC1, b1, fmaf(kC7, b2, kC3 * b3)));
+    x[7] = 0.5f * fmaf(kC7, b0, fmaf(-kC5, b1, fmaf(kC3, b2, -kC1 * b3)));
+}
+
+__device__ __forceinline__ void idct8(float* x) {
+    const float e0 = (x[0] + x[4]) * kS8, e1 = (x[0] - x[4]) * kS8;
+    const float o0 = fmaf(0.5f * kC2, x[2], 0.5f * kC6 * x[6]);
+    const float o1 = fmaf(0.5f * kC6, x[2], -0.5f * kC2 * x[6]);
+    const float a0 = e0 + o0, a3 = e0 - o0, a1 = e1 + o1, a2 = e1 - o1;
+    const float X1 = 0.5f * x[1], X3 = 0.5f * x[3], X5 = 0.5f * x[5], X7 = 0.5f * x[7];
+    const float b0 = fmaf(kC1, X1, fmaf(kC3, X3, fmaf(kC5, X5, kC7 * X7)));
+    const float b1 = fmaf(kC3, X1, fmaf(-kC7, X3, fmaf(-kC1, X5, -kC5 * X7)));
+    const float b2 = fmaf(kC5, X1, fmaf(-kC1, X3, fmaf(kC7, X5, kC3 * X7)));
+    const float b3 = fmaf(kC7, X1, fmaf(-kC5, X3, fmaf(kC3, X5, -kC1 * X7)));
+    x[0] = a0 + b0;
+    x[7] = a0 - b0;
+    x[1] = a1 + b1;
+    x[6] = a1 - b1;
+    x[2] = a2 + b2;
+    x[5] = a2 - b2;
+    x[3] = a3 + b3;
+    x[4] = a3 - b3;
+}
+
+template <int G>
+__device__ __forceinline__ float haar_scale_c(int j) {
+    int e = 0;
+    if (j == 0) {
+        while ((1 << e) < G) ++e;
+    } else {
+        while (((j >> e) & 1) == 0) ++e;
+        ++e;
+    }
+    float f = 1.f;
+    for (int i = 0; i < e / 2; ++i) f *= 0.5f;
+    return e % 2 ? f * 0.70710678118654752f : f;
+}
+
+// in-place orthonormal Haar of G samples (dct8.cpp:601-642 layout)
+template <int G>
+__device__ __forceinline__ void haar_fwd(float* t) {
+#pragma unroll
+    for (int h = 1; h < G; h <<= 1)
+#pragma unroll
+        for (int i = 0; i < G; i += 2 * h) {
+            const float a = t[i], b = t[i + h];
+            t[i] = a + b;
+            t[i + h] = a - b;
+        }
+#pragma unroll
+    for (int j = 0; j < G; ++j) t[j] *= haar_scale_c<G>(j);
+}
+
+template <int G>
+__device__ __forceinline__ void haar_inv(float* t) {
+#pragma unroll
+    for (int j = 0; j < G; ++j) t[j] *= haar_scale_c<G>(j);
+#pragma unroll
+    for (int h = G / 2; h >= 1; h >>= 1)
+#pragma unroll
+        for (int i = 0; i < G; i += 2 * h) {
+            const float a = t[i], b = t[i + h];
+            t[i] = a + b;
+            t[i + h] = a - b;
+        }
+}
+
+constexpr int kWarps = 4;
+
+template <int G>
+struct Shape {
+    static constexpr int LP = 32 / G;      // lanes per patch
+    static constexpr int RPL = 8 / LP;     // rows (and columns) per lane
+    static constexpr int S = 64 + LP;      // patch stride in the shared cube
+};
+
+// rows -> (DCT on rows) -> cube, cube -> columns -> (DCT) -> cube
+template <int G, bool INV>
+__device__ __forceinline__ void col_pass(float* cube, int g, int q) {
+    using Sh = Shape<G>;
+#pragma unroll
+    for (int t = 0; t < Sh::RPL; ++t) {
+        const int c = q + Sh::LP * t;
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + i * 8 + c];
+        if (INV)
+            idct8(v);
+        else
+            fdct8(v);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cube[g * Sh::S + i * 8 + c] = v[i];
+    }
+}
+
+// One group on one warp. Acc(s) gives the (num, wsum, stride) of slot s,
+// Src(s, row, x) / Ref(s, row, x) the source rows.
+template <int G, bool WIENER, class SrcRow, class RefRow, class AccOf>
+__device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane, int k, int32_t p, int s,
+                                             float sigma, SrcRow src_row, RefRow ref_row, AccOf acc_of) {
+    using Sh = Shape<G>;
+    const int g = lane / Sh::LP, q = lane % Sh::LP;
+    const int px = pos_x(p), py = pos_y(p);
+    // gather and row transforms
+#pragma unroll
+    for (int r = 0; r < Sh::RPL; ++r) {
+        const int row = q * Sh::RPL + r;
+        float v[8], w[8];
+        if (g < k) {
+            const float* sp = src_row(s, py + row) + px;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = __ldg(sp + j);
+            if (WIENER) {
+                const float* rp = ref_row(s, py + row) + px;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) w[j] = __ldg(rp + j);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = w[j] = 0.f;
+        }
+        fdct8(v);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) cube[g * Sh::S + row * 8 + j] = v[j];
+        if (WIENER) {
+            fdct8(w);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) rcube[g * Sh::S + row * 8 + j] = w[j];
+        }
+    }
+    __syncwarp();
+    col_pass<G, false>(cube, g, q);
+    if (WIENER) col_pass<G, false>(rcube, g, q);
+    __syncwarp();
+    // Haar tubes, shrinkage, inverse Haar: positions lane and lane + 32
+    int kept = 0;
+    float w2 = 0.f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int f = lane + 32 * h;
+        float t[G];
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg) t[gg] = cube[gg * Sh::S + f];
+        haar_fwd<G>(t);
+        if (WIENER) {
+            float r[G];
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) r[gg] = rcube[gg * Sh::S + f];
+            haar_fwd<G>(r);
+            const float sig2 = sigma * sigma;
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                float wt = 1.f;
+                if (!(gg == 0 && f == 0)) {
+                    const float r2 = r[gg] * r[gg];
+                    const float den = r2 + sig2;
+                    wt = den > 0.f ? __fdiv_rn(r2, den) : 0.f;
+                }
+                t[gg] *= wt;
+                w2 = fmaf(wt, wt, w2);
+            }
+        } else {
+            const float thr = 2.7f * sigma;
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                if (!(gg == 0 && f == 0) && fabsf(t[gg]) < thr) {
+                    t[gg] = 0.f;
+                } else {
+                    ++kept;
+                }
+            }
+        }
+        haar_inv<G>(t);
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg) cube[gg * Sh::S + f] = t[gg];
+    }
+    float weight;
+    if (WIENER) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w2 += __shfl_xor_sync(0xffffffffu, w2, o);
+        weight = __fdiv_rn(1.f, fmaxf(w2, 1e-12f));
+    } else {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+        weight = __fdiv_rn(1.f, (float)(kept > 1 ? kept : 1));
+    }
+    __syncwarp();
+    col_pass<G, true>(cube, g, q);
+    __syncwarp();
+    if (g < k) {
+        long long* num;
+        long long* wsum;
+        int64_t as;
+        acc_of(s, num, wsum, as);
+#pragma unroll
+        for (int r = 0; r < Sh::RPL; ++r) {
+            const int row = q * Sh::RPL + r;
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + row * 8 + j];
+            idct8(v);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(num + (int64_t)(py + row) * as + px);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                atomicAdd(dst + j, (unsigned long long)__double2ll_rn((double)weight * (double)v[j] * kFixedScale));
+        }
+        if (q == 0)
+            atomicAdd(reinterpret_cast<unsigned long long*>(wsum + (int64_t)py * as + px),
+                      (unsigned long long)__double2ll_rn((double)weight * kFixedScale));
+    }
+    __syncwarp();
+}
+
+// Temporal / single-plane form: slots of GroupIO.
+template <int G, bool WIENER>
+__global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const int32_t* __restrict__ pos,
+                                                             const int32_t* __restrict__ slot,
+                                                             const int32_t* __restrict__ count, int njobs,
+                                                             float sigma) {
+    using Sh = Shape<G>;
+    constexpr int CUBE = G * Sh::S;
+    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / Sh::LP;
+    const int stride_w = gridDim.x * kWarps;
+    for (int job = blockIdx.x * kWarps + warp; job < njobs; job += stride_w) {
+        const int k = count[job];
+        if (k <= 0) continue;
+        const int32_t p = g < k ? pos[(size_t)job * G + g] : 0;
+        const int s = (slot && g < k) ? slot[(size_t)job * G + g] : 0;
+        filter_group<G, WIENER>(
+            smem[warp], smem[warp] + CUBE, lane, k, p, s, sigma,
+            [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
+            [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
+            [&](int sl, long long*& num, long long*& wsum, int64_t& as) {
+                num = io.num[sl];
+                wsum = io.wsum[sl];
+                as = io.acc_stride;
+            });
+    }
+}
+
+// Batched form: every job of every plane of the batch, a warp per group.
+template <int G, bool WIENER>
+__global__ void __launch_bounds__(32 * kWarps) group8_batch_kernel(const __grid_constant__ GroupBatch gb) {
+    using Sh = Shape<G>;
+    constexpr int CUBE = G * Sh::S;
+    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / Sh::LP;
+    const int stride_w = gridDim.x * kWarps;
+    int pl = 0;
+    for (int job = blockIdx.x * kWarps + warp; job < gb.total_jobs; job += stride_w) {
+        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= job) ++pl;
+        const GroupPlane& P_ = gb.p[pl];
+        const int lj = job - P_.job0;
+        const int k = P_.count[lj];
+        if (k <= 0) continue;
+        const int32_t p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
+        filter_group<G, WIENER>(
+            smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma,
+            [&](int, int row) { return P_.src + (int64_t)row * P_.stride; },
+            [&](int, int row) { return P_.ref + (int64_t)row * P_.ref_stride; },
+            [&](int, long long*& num, long long*& wsum, int64_t& as) {
+                num = P_.num;
+                wsum = P_.wsum;
+                as = P_.acc_stride;
+            });
+    }
+}
+
+template <int G, bool W>
+void launch_gw(const GroupIO& io, const int32_t* pos, const int32_t* slot, const int32_t* count, int njobs,
+               float sigma, cudaStream_t stream) {
+    const int blocks = std::min(ceil_div(njobs, kWarps), 148 * 16);
+    group8_kernel<G, W><<<blocks, 32 * kWarps, 0, stream>>>(io, pos, slot, count, njobs, sigma);
+    NSSB_CUDA(cudaGetLastError());
+}
+
+template <int G, bool W>
+void launch_batch_gw(const GroupBatch& gb, cudaStream_t stream) {
+    const int blocks = std::min(ceil_div(gb.total_jobs, kWarps), 148 * 16);
+    group8_batch_kernel<G, W><<<blocks, 32 * kWarps, 0, stream>>>(gb);
+    NSSB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, const int32_t* count, int njobs,
+                   int group, float sigma, bool wiener, cudaStream_t stream) {
+    if (njobs <= 0) return true;
+    switch (group) {
+        case 4:
+            wiener ? launch_gw<4, true>(io, pos, slot, count, njobs, sigma, stream)
+                   : launch_gw<4, false>(io, pos, slot, count, njobs, sigma, stream);
+            return true;
+        case 8:
+            wiener ? launch_gw<8, true>(io, pos, slot, count, njobs, sigma, stream)
+                   : launch_gw<8, false>(io, pos, slot, count, njobs, sigma, stream);
+            return true;
+        case 16:
+            wiener ? launch_gw<16, true>(io, pos, slot, count, njobs, sigma, stream)
+                   : launch_gw<16, false>(io, pos, slot, count, njobs, sigma, stream);
+            return true;
+        default:
+            return false;
+    }
+}
+
+bool launch_group8_batch(const GroupBatch& gb, int group, bool wiener, cudaStream_t stream) {
+    if (gb.total_jobs <= 0) return true;
+    switch (group) {
+        case 4: wiener ? launch_batch_gw<4, true>(gb, stream) : launch_batch_gw<4, false>(gb, stream); return true;
+        case 8: wiener ? launch_batch_gw<8, true>(gb, stream) : launch_batch_gw<8, false>(gb, stream); return true;
+        case 16: wiener ? launch_batch_gw<16, true>(gb, stream) : launch_batch_gw<16, false>(gb, stream); return true;
+        default: return false;
+    }
+}
+
+}  // namespace nssb

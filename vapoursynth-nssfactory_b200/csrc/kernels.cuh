@@ -1,0 +1,119 @@
+// Kernel launchers of the BM3D path (sm_100a). All device pointers; strides in
+// elements; every launcher enqueues on `stream` and returns immediately.
+#pragma once
+
+#include "common.cuh"
+
+#include <cstdint>
+
+namespace nssb {
+
+constexpr int kMaxSlots = 33;  // 2 * 16 + 1 temporal slots
+
+// Spatial matching of the whole raster grid of one plane (see nss_b200.h).
+void launch_match_spatial(const float* plane, int64_t stride, int width, int height, int block, int step,
+                          int bm_range, int group, int32_t* pos, float* dist, int32_t* count, cudaStream_t stream);
+
+// A batch of planes sharing one stage shape, processed by one launch per
+// kernel (the planes of a frame, or of many frames in the batched form).
+constexpr int kMaxBatchPlanes = 192;
+struct MatchPlane {
+    const float* src;  // match source plane
+    int64_t stride;
+    int32_t* pos;      // njobs x group
+    float* dist;       // njobs x group, or null
+    int32_t* count;    // njobs
+    int W, H, nx, ny;
+    int cta0;          // first CTA of this plane in the launch
+};
+struct MatchBatch {
+    int n, step;
+    MatchPlane p[kMaxBatchPlanes];
+};
+// The specialised exact matcher for 8x8 blocks (match8.cu) over a batch of
+// planes; false when the shape (bm_range, group, step) has no specialisation.
+bool launch_match8_batch(MatchBatch& batch, int bm_range, int group, cudaStream_t stream);
+bool launch_match8(const float* plane, int64_t stride, int width, int height, int step, int bm_range, int group,
+                   int32_t* pos, float* dist, int32_t* count, cudaStream_t stream);
+
+struct GroupPlane {
+    const float* src;
+    const float* ref;  // Wiener reference, or null
+    int64_t stride, ref_stride;
+    long long* num;
+    long long* wsum;
+    int64_t acc_stride;
+    const int32_t* pos;
+    const int32_t* count;
+    int job0, njobs;
+    float sigma;
+};
+struct GroupBatch {
+    int n, total_jobs;
+    GroupPlane p[kMaxBatchPlanes];
+};
+// Warp-per-group filter for 8x8 blocks and groups of 4/8/16 over a batch of
+// planes (all Wiener or all hard threshold); false when the shape has none.
+bool launch_group8_batch(const GroupBatch& batch, int group, bool wiener, cudaStream_t stream);
+
+struct FinishPlane {
+    long long* num;          // cleared by the kernel after use
+    const long long* wsum;
+    int64_t acc_stride;
+    const float* src;
+    int64_t sstride;
+    float* dst;
+    int64_t dstride;
+    int W, H, tiles_x, cta0;
+};
+struct FinishBatch {
+    int n, block, total_ctas;
+    FinishPlane p[kMaxBatchPlanes];
+};
+void launch_finish_batch(const FinishBatch& batch, cudaStream_t stream);
+int finish_tiles_x(int w);
+int finish_tiles(int w, int h);
+
+// Predictive temporal layers on top of a spatial result already in pos/dist/count
+// (slot t0). Fills slot[] and extends each group across the valid slots.
+struct TemporalPlanes {
+    const float* plane[kMaxSlots];
+    int64_t stride[kMaxSlots];
+};
+void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int valid_begin, int valid_end,
+                           int width, int height, int block, int step, int group, int ps_num, int ps_range,
+                           int32_t* pos, int32_t* slot, float* dist, int32_t* count, cudaStream_t stream);
+
+// Group filtering + aggregation of one stage (hard threshold, or Wiener when
+// ref planes are given). Sums go to fixed-point num (per pixel) and wsum (per
+// patch origin) of the slot each patch came from.
+struct GroupIO {
+    const float* src[kMaxSlots];
+    const float* ref[kMaxSlots];  // Wiener reference planes (nullptr: hard threshold)
+    int64_t stride;               // element stride of src planes
+    int64_t ref_stride;           // element stride of ref planes
+    long long* num[kMaxSlots];
+    long long* wsum[kMaxSlots];
+    int64_t acc_stride;           // element stride of num/wsum
+};
+void launch_group_filter(const GroupIO& io, int width, int height, const int32_t* pos, const int32_t* slot,
+                         const int32_t* count, int njobs, int block, int group, float sigma, bool wiener,
+                         float* scratch, size_t scratch_floats, cudaStream_t stream);
+// The specialised warp-per-group filter for 8x8 blocks and groups of 4/8/16
+// (group8.cu); false when the shape has none.
+bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, const int32_t* count, int njobs,
+                   int group, float sigma, bool wiener, cudaStream_t stream);
+// Device scratch (floats) the generic group kernel needs for this shape, 0 if none.
+size_t group_filter_scratch_floats(int block, int group, bool wiener);
+
+// out = den > 1e-12 ? num / den : src, den the B x B box sum of the origin
+// weights; num and wsum are read, not cleared.
+void launch_finish(const long long* num, const long long* wsum, int64_t acc_stride, const float* src,
+                   int64_t sstride, float* dst, int64_t dstride, int width, int height, int block,
+                   cudaStream_t stream);
+
+// The legacy fat slice of one target: num and den as float planes.
+void launch_fat_slice(const long long* num, const long long* wsum, int64_t acc_stride, float* dst_num,
+                      float* dst_den, int64_t dstride, int width, int height, int block, cudaStream_t stream);
+
+}  // namespace nssb
