@@ -33,15 +33,25 @@ float om_noise_effective(float user_sigma) {
 
 /* ---------------------------------------------------------------- distances */
 
+/* The SSD order of this build: the block's left columns [0, B/2) and right
+ * columns [B/2, B) each take one FMA chain in row-major order, and the two
+ * chains are added once: lo + hi. */
 float om_ssd(const float* a, ptrdiff_t sa, const float* b, ptrdiff_t sb, int block) {
-    float acc = 0.f;
+    const int h = block >> 1;
+    float lo = 0.f, hi = 0.f;
     for (int i = 0; i < block; ++i) {
-        for (int j = 0; j < block; ++j) {
+        for (int j = 0; j < h; ++j) {
             const float d = a[i * sa + j] - b[i * sb + j];
-            acc = fmaf(d, d, acc);
+            lo = fmaf(d, d, lo);
         }
     }
-    return acc;
+    for (int i = 0; i < block; ++i) {
+        for (int j = h; j < block; ++j) {
+            const float d = a[i * sa + j] - b[i * sb + j];
+            hi = fmaf(d, d, hi);
+        }
+    }
+    return lo + hi;
 }
 
 /* The 8-lane tree of SpatialMatch8 (ssd.cpp:207-237): lane j accumulates rows
@@ -137,46 +147,57 @@ int om_grid_pos(int i, int extent, int block, int step) { return imin(i * step, 
  * independent, so the compiler's vector form gives om_ssd's bits. */
 static void ssd_span(const float* refblk, int block, const float* buf, ptrdiff_t bstride, int n, int nrows,
                      float* out, int ostride) {
-    /* nrows (<= 4) candidate rows x n candidates; candidate row q starts at buffer row q */
+    /* nrows (<= 2) candidate rows x n candidates; candidate row q starts at
+     * buffer row q. Left and right half-column chains as in om_ssd. */
+    const int h = block >> 1;
     for (int c0 = 0; c0 < n; c0 += 24) {
-        float acc[4][24];
+        float lo[2][24], hi[2][24];
 #if defined(__AVX2__) && defined(__FMA__)
         /* vfmadd is the exactly rounded fma: the same bits as fmaf */
-        __m256 a[4][3];
-        for (int q = 0; q < 4; ++q)
-            for (int v = 0; v < 3; ++v) a[q][v] = _mm256_setzero_ps();
+        __m256 a[2][3], b[2][3];
+        for (int q = 0; q < 2; ++q)
+            for (int v = 0; v < 3; ++v) a[q][v] = b[q][v] = _mm256_setzero_ps();
         for (int i = 0; i < block; ++i) {
             for (int j = 0; j < block; ++j) {
                 const __m256 r = _mm256_set1_ps(refblk[i * block + j]);
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < 2; ++q) {
                     const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
                     for (int v = 0; v < 3; ++v) {
                         const __m256 d = _mm256_sub_ps(r, _mm256_loadu_ps(row + 8 * v));
-                        a[q][v] = _mm256_fmadd_ps(d, d, a[q][v]);
+                        if (j < h)
+                            a[q][v] = _mm256_fmadd_ps(d, d, a[q][v]);
+                        else
+                            b[q][v] = _mm256_fmadd_ps(d, d, b[q][v]);
                     }
                 }
             }
         }
-        for (int q = 0; q < 4; ++q)
-            for (int v = 0; v < 3; ++v) _mm256_storeu_ps(acc[q] + 8 * v, a[q][v]);
+        for (int q = 0; q < 2; ++q)
+            for (int v = 0; v < 3; ++v) {
+                _mm256_storeu_ps(lo[q] + 8 * v, a[q][v]);
+                _mm256_storeu_ps(hi[q] + 8 * v, b[q][v]);
+            }
 #else
-        for (int q = 0; q < 4; ++q)
-            for (int c = 0; c < 24; ++c) acc[q][c] = 0.f;
+        for (int q = 0; q < 2; ++q)
+            for (int c = 0; c < 24; ++c) lo[q][c] = hi[q][c] = 0.f;
         for (int i = 0; i < block; ++i)
             for (int j = 0; j < block; ++j) {
                 const float r = refblk[i * block + j];
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < 2; ++q) {
                     const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
                     for (int c = 0; c < 24; ++c) {
                         const float d = r - row[c];
-                        acc[q][c] = fmaf(d, d, acc[q][c]);
+                        if (j < h)
+                            lo[q][c] = fmaf(d, d, lo[q][c]);
+                        else
+                            hi[q][c] = fmaf(d, d, hi[q][c]);
                     }
                 }
             }
 #endif
         const int m = n - c0 < 24 ? n - c0 : 24;
         for (int q = 0; q < nrows; ++q)
-            for (int c = 0; c < m; ++c) out[q * ostride + c0 + c] = acc[q][c];
+            for (int c = 0; c < m; ++c) out[q * ostride + c0 + c] = lo[q][c] + hi[q][c];
     }
 }
 
@@ -208,11 +229,11 @@ int om_spatial_match(const float* plane, ptrdiff_t stride, int width, int height
         if (valid) memcpy(dst, plane + (ptrdiff_t)(top + r) * stride + left, (size_t)valid * sizeof(float));
         memset(dst + valid, 0, (size_t)(bstride - valid) * sizeof(float));
     }
-    float dist[4][2 * 64 + 1 + 24];
+    float dist[2][2 * 64 + 1 + 24];
     for (int y = top; y <= bottom; ++y) {
-        const int q = (y - top) & 3;
+        const int q = (y - top) & 1;
         if (q == 0 && !(lanes8 && block == 8))
-            ssd_span(refblk, block, buf + (ptrdiff_t)(y - top) * bstride, bstride, span, imin(4, bottom - y + 1),
+            ssd_span(refblk, block, buf + (ptrdiff_t)(y - top) * bstride, bstride, span, imin(2, bottom - y + 1),
                      dist[0], 2 * 64 + 1 + 24);
         if (lanes8 && block == 8) {
             for (int c = 0; c < span; ++c)

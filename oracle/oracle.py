@@ -181,14 +181,16 @@ def bm3d_plane(src, st: Stage, ref=None, want_matches=False):
     return dst
 
 
-def bm3d_planes_chroma(planes, st: Stage, refs=None):
-    """CBM3D: groups matched on plane 0 (of refs when given) filter every plane."""
+def bm3d_planes_chroma(planes, stages, refs=None):
+    """CBM3D: groups matched on plane 0 (of refs when given) filter every plane;
+    stages: one Stage per plane (its sigma; the shape of plane 0 holds for all)."""
     ps = [_f32(p) for p in planes]
     rs = [_f32(p) for p in refs] if refs is not None else None
     h, w = ps[0].shape
     match = rs[0] if rs is not None else ps[0]
     outs = []
     for c, p in enumerate(ps):
+        st = stages[c]
         dst = np.empty_like(p)
         r = rs[c] if rs is not None else None
         if st.sigma == 0.0:

@@ -167,14 +167,13 @@ def test_frame_api_chroma(nssb, oracle, synth, dev):
     # plane 0 exactly as without chroma; every plane filtered with the plane-0 groups
     alone = nssb.BM3D(nssb.Clip.from_frames([(y,)], nssb.GRAY), sigma=10).get_frame(0)
     assert np.array_equal(got[0], alone[0])
-    for c, sg in enumerate((10.0, 6.0, 6.0)):
-        st = oracle.stage(oracle.effective_sigma(sg))
-        want = oracle.bm3d_planes_chroma([y, u, v], st)[c]
-        assert oracle.psnr(got[c], want) >= MIN_PSNR
+    stages = [oracle.stage(oracle.effective_sigma(sg)) for sg in (10.0, 6.0, 6.0)]
+    want = oracle.bm3d_planes_chroma([y, u, v], stages)
+    for c in range(3):
+        assert oracle.psnr(got[c], want[c]) >= MIN_PSNR
     # two-stage CBM3D: plane 0 of the basic estimate guides the Wiener stage
     both = nssb.BM3D(clip, sigma=[10, 6, 6], chroma=1, final=1).get_frame(0)
-    for c, sg in enumerate((10.0, 6.0, 6.0)):
-        st = oracle.stage(oracle.effective_sigma(sg))
-        basic = oracle.bm3d_planes_chroma([y, u, v], st)
-        want = oracle.bm3d_planes_chroma([y, u, v], st, refs=basic)[c]
-        assert oracle.psnr(both[c], want) >= MIN_PSNR
+    basic = oracle.bm3d_planes_chroma([y, u, v], stages)
+    want = oracle.bm3d_planes_chroma([y, u, v], stages, refs=basic)
+    for c in range(3):
+        assert oracle.psnr(both[c], want[c]) >= MIN_PSNR

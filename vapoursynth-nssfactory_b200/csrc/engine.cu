@@ -252,11 +252,14 @@ void Engine::run_stage(StageItem* items, int n) {
             gbatch_.p[gbatch_.n++] = GroupPlane{it.src, it.ref, it.sstride, it.rstride, ac.num, ac.wsum, ac.pitch,
                                                 it.shared_pos ? it.shared_pos : sc.pos,
                                                 it.shared_count ? it.shared_count : sc.count, gbatch_.total_jobs, jobs,
-                                                it.sp->sigma};
+                                                it.sp->sigma, w, h, 0};
             gbatch_.total_jobs += jobs;
         }
         bool gok = false;
-        if (sp.block == 8) timed(kGroup, [&] { gok = launch_group8_batch(gbatch_, sp.group, wiener, stream_); });
+        if (sp.block == 8)
+            timed(kGroup, [&] {
+                gok = launch_group8_batch(gbatch_, sp.group, wiener, stream_);
+            });
         if (!gok) {
             for (int q = 0; q < gbatch_.n; ++q) {
                 const GroupPlane& g = gbatch_.p[q];

@@ -74,12 +74,16 @@ __global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restri
     dden[(int64_t)y * ds + x] = (float)((double)den[r][c] * kFixedInv);
 }
 
-// Batched finish over a plane table; num is cleared as it is consumed (each
-// pixel's num is read by exactly one thread), so the next stage finds it zero.
-__global__ void __launch_bounds__(kTX* kTY) finish_batch_kernel(const __grid_constant__ FinishBatch fb) {
-    __shared__ long long wt[kTY + kMaxB - 1][kTX + kMaxB - 1];
-    __shared__ long long hs[kTY + kMaxB - 1][kTX];
-    __shared__ long long den[kTY][kTX];
+// Batched finish over a plane table. A CTA finishes a 64 x 32 tile, 8
+// pixels per thread (one column, 8 rows): the origin weights of the tile and
+// its (B-1)-pixel halo, num and src are all requested before the first
+// barrier; den comes from sliding B-wide row sums, then B-tall column sums,
+// exact in int64. num is cleared as it is consumed (each pixel's num is read
+// by exactly one thread), so the next stage finds it zero.
+constexpr int kFX = 64, kFY = 32, kFT = 256;
+
+__global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant__ FinishBatch fb) {
+    extern __shared__ long long fsm[];  // wt[(kFY + B - 1)][(kFX + B - 1)], then hs[(kFY + B - 1)][kFX]
     int pl = 0;
     {
         int lo = 0, hi = fb.n - 1;
@@ -90,32 +94,75 @@ __global__ void __launch_bounds__(kTX* kTY) finish_batch_kernel(const __grid_con
         pl = lo;
     }
     const FinishPlane& P = fb.p[pl];
+    const int B = fb.block;
     const int local = blockIdx.x - P.cta0;
     const int ty = local / P.tiles_x, tx = local - ty * P.tiles_x;
-    const int x0 = tx * kTX, y0 = ty * kTY;
-    box_den(P.wsum, P.acc_stride, P.W, P.H, fb.block, x0, y0, wt, hs, den);
-    const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
-    const int x = x0 + c, y = y0 + r;
-    if (x >= P.W || y >= P.H) return;
-    const long long d = den[r][c];
-    long long* np = P.num + (int64_t)y * P.acc_stride + x;
-    const long long nv = *np;
-    *np = 0;
-    const double dd = (double)d * kFixedInv;
-    P.dst[(int64_t)y * P.dstride + x] = (float)dd > 1e-12f ? (float)((double)nv / (double)d)
-                                                           : P.src[(int64_t)y * P.sstride + x];
+    const int x0 = tx * kFX, y0 = ty * kFY;
+    const int c = threadIdx.x & (kFX - 1), q = threadIdx.x / kFX;  // column, 8-row quarter
+    const int x = x0 + c;
+    // this thread's num and src, requested first
+    long long nv[8];
+    float sv[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int y = y0 + q * 8 + r;
+        const bool ok = x < P.W && y < P.H;
+        nv[r] = ok ? P.num[(int64_t)y * P.acc_stride + x] : 0;
+        sv[r] = ok ? P.src[(int64_t)y * P.sstride + x] : 0.f;
+    }
+    const int rows = kFY + B - 1, cols = kFX + B - 1;
+    long long* wtp = fsm;
+    long long* hsp = fsm + rows * cols;
+#define wt(r, cc) wtp[(r) * cols + (cc)]
+#define hs(r, cc) hsp[(r) * kFX + (cc)]
+    for (int i = threadIdx.x; i < rows * cols; i += kFT) {
+        const int r = i / cols, cc = i - r * cols;
+        const int yy = y0 - B + 1 + r, xx = x0 - B + 1 + cc;
+        wt(r, cc) = (yy >= 0 && yy < P.H && xx >= 0 && xx < P.W) ? P.wsum[(int64_t)yy * P.acc_stride + xx] : 0ll;
+    }
+    __syncthreads();
+    // row sums: 8 consecutive columns of one row per task, sliding
+    for (int t = threadIdx.x; t < rows * (kFX / 8); t += kFT) {
+        const int r = t / (kFX / 8), c0 = (t - r * (kFX / 8)) * 8;
+        long long sum = 0;
+        for (int k = 0; k < B; ++k) sum += wt(r, c0 + k);
+        hs(r, c0) = sum;
+#pragma unroll
+        for (int j = 1; j < 8; ++j) {
+            sum += wt(r, c0 + j + B - 1) - wt(r, c0 + j - 1);
+            hs(r, c0 + j) = sum;
+        }
+    }
+    __syncthreads();
+    // column sums down this thread's 8 rows, then the finish
+    long long den = 0;
+    for (int k = 0; k < B; ++k) den += hs(q * 8 + k, c);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r > 0) den += hs(q * 8 + r + B - 1, c) - hs(q * 8 + r - 1, c);
+        const int y = y0 + q * 8 + r;
+        if (x < P.W && y < P.H) {
+            P.num[(int64_t)y * P.acc_stride + x] = 0;
+            const float dd = (float)((double)den * kFixedInv);
+            P.dst[(int64_t)y * P.dstride + x] = dd > 1e-12f ? (float)((double)nv[r] / (double)den) : sv[r];
+        }
+    }
+#undef wt
+#undef hs
 }
 
 }  // namespace
 
 void launch_finish_batch(const FinishBatch& fb, cudaStream_t stream) {
     if (fb.total_ctas <= 0) return;
-    finish_batch_kernel<<<fb.total_ctas, kTX * kTY, 0, stream>>>(fb);
+    const size_t smem = (size_t)(kFY + fb.block - 1) * (kFX + fb.block - 1 + kFX) * sizeof(long long);
+    NSSB_CUDA(cudaFuncSetAttribute(finish_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    finish_batch_kernel<<<fb.total_ctas, kFT, smem, stream>>>(fb);
     NSSB_CUDA(cudaGetLastError());
 }
 
-int finish_tiles_x(int w) { return ceil_div(w, kTX); }
-int finish_tiles(int w, int h) { return ceil_div(w, kTX) * ceil_div(h, kTY); }
+int finish_tiles_x(int w) { return ceil_div(w, kFX); }
+int finish_tiles(int w, int h) { return ceil_div(w, kFX) * ceil_div(h, kFY); }
 
 void launch_finish(const long long* num, const long long* wsum, int64_t acc_stride, const float* src,
                    int64_t sstride, float* dst, int64_t dstride, int width, int height, int block,

@@ -131,9 +131,10 @@ __device__ __forceinline__ void col_pass(float* cube, int g, int q) {
 
 // One group on one warp. Acc(s) gives the (num, wsum, stride) of slot s,
 // Src(s, row, x) / Ref(s, row, x) the source rows.
-template <int G, bool WIENER, class SrcRow, class RefRow, class AccOf>
+template <int G, bool WIENER, class SrcRow, class RefRow, class AddNum, class AddWeight>
 __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane, int k, int32_t p, int s,
-                                             float sigma, SrcRow src_row, RefRow ref_row, AccOf acc_of) {
+                                             float sigma, SrcRow src_row, RefRow ref_row, AddNum add_num,
+                                             AddWeight add_weight) {
     using Sh = Shape<G>;
     const int g = lane / Sh::LP, q = lane % Sh::LP;
     const int px = pos_x(p), py = pos_y(p);
@@ -223,26 +224,33 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
     __syncwarp();
     col_pass<G, true>(cube, g, q);
     __syncwarp();
-    if (g < k) {
-        long long* num;
-        long long* wsum;
-        int64_t as;
-        acc_of(s, num, wsum, as);
+    // inverse row transforms back into the cube
 #pragma unroll
-        for (int r = 0; r < Sh::RPL; ++r) {
-            const int row = q * Sh::RPL + r;
-            float v[8];
+    for (int r = 0; r < Sh::RPL; ++r) {
+        const int row = q * Sh::RPL + r;
+        float v[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + row * 8 + j];
-            idct8(v);
-            unsigned long long* dst = reinterpret_cast<unsigned long long*>(num + (int64_t)(py + row) * as + px);
+        for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + row * 8 + j];
+        idct8(v);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                atomicAdd(dst + j, (unsigned long long)__double2ll_rn((double)weight * (double)v[j] * kFixedScale));
+        for (int j = 0; j < 8; ++j) cube[g * Sh::S + row * 8 + j] = v[j];
+    }
+    if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn((double)weight * kFixedScale));
+    __syncwarp();
+    // aggregation with 8 consecutive lanes on 8 consecutive pixels of a row:
+    // a warp instruction covers 4 rows x 8 columns of one patch
+#pragma unroll
+    for (int t = 0; t < 2 * G; ++t) {
+        const int e = t * 32 + lane, gg = e >> 6, i = (e >> 3) & 7, j = e & 7;
+        if (gg < k) {
+            const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
+            const int ss = __shfl_sync(0xffffffffu, s, gg * Sh::LP);
+            add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
+                    __double2ll_rn((double)weight * (double)cube[gg * Sh::S + i * 8 + j] * kFixedScale));
+        } else {
+            (void)__shfl_sync(0xffffffffu, p, 0);
+            (void)__shfl_sync(0xffffffffu, s, 0);
         }
-        if (q == 0)
-            atomicAdd(reinterpret_cast<unsigned long long*>(wsum + (int64_t)py * as + px),
-                      (unsigned long long)__double2ll_rn((double)weight * kFixedScale));
     }
     __syncwarp();
 }
@@ -268,10 +276,13 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
             smem[warp], smem[warp] + CUBE, lane, k, p, s, sigma,
             [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
             [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
-            [&](int sl, long long*& num, long long*& wsum, int64_t& as) {
-                num = io.num[sl];
-                wsum = io.wsum[sl];
-                as = io.acc_stride;
+            [&](int sl, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(io.num[sl] + (int64_t)y * io.acc_stride + x),
+                          (unsigned long long)v);
+            },
+            [&](int sl, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
+                          (unsigned long long)v);
             });
     }
 }
@@ -297,10 +308,13 @@ __global__ void __launch_bounds__(32 * kWarps) group8_batch_kernel(const __grid_
             smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma,
             [&](int, int row) { return P_.src + (int64_t)row * P_.stride; },
             [&](int, int row) { return P_.ref + (int64_t)row * P_.ref_stride; },
-            [&](int, long long*& num, long long*& wsum, int64_t& as) {
-                num = P_.num;
-                wsum = P_.wsum;
-                as = P_.acc_stride;
+            [&](int, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(P_.num + (int64_t)y * P_.acc_stride + x),
+                          (unsigned long long)v);
+            },
+            [&](int, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(P_.wsum + (int64_t)y * P_.acc_stride + x),
+                          (unsigned long long)v);
             });
     }
 }

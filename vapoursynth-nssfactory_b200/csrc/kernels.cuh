@@ -47,6 +47,8 @@ struct GroupPlane {
     const int32_t* count;
     int job0, njobs;
     float sigma;
+    int W, H;   // plane size
+    int cta0;   // first CTA of this plane
 };
 struct GroupBatch {
     int n, total_jobs;

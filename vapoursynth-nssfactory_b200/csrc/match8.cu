@@ -1,20 +1,23 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
-// row-major FMA chain per candidate, keys dist << 32 | y << 16 | x); only the
-// schedule differs:
-//   - a CTA is 32 consecutive references of one grid row (one per lane) of
-//     one plane of a batch; its P warps split the 2R+1 window columns, each
-//     lane holding its reference block in 64 registers;
-//   - the CTA stages the 2R+8 rows of its windows once in shared memory with a
-//     skewed layout (column c at c + c/32), so 32 lanes whose references sit
-//     8 columns apart read 32 different banks;
-//   - a lane walks its columns one by one: the column's 2R+8 image rows stream
-//     through and each row is applied to the 8 candidates that overlap it.
-//     Candidate k lives in accumulator k & 7; with the row loop unrolled the
-//     slots are register names, so a row costs 8 shared loads and 64
-//     subtract/FMA pairs. A finished candidate enters the lane's register
-//     top-k; the P partial lists of a reference merge in shared memory.
+// keys dist << 32 | y << 16 | x, and this build's SSD order: left columns
+// 0-3 and right columns 4-7 each one FMA chain in row-major order, then
+// lo + hi); only the schedule differs:
+//   - a CTA is 32 consecutive references of one grid row of one plane of a
+//     batch. Two lanes serve each reference, one per column half, each with
+//     its 8x4 half block in 32 registers; a warp is 16 references x 2 halves
+//     and the CTA's P warp pairs split the 2R+1 window columns;
+//   - the CTA stages the 2R+8 rows of its windows once in shared memory, the
+//     column c of a row stored at c ^ ((c >> 5) & 3): the 32 lanes read 32
+//     columns 4 apart, which this swizzle sends to 32 different banks;
+//   - a lane walks its window columns one by one: the column's 2R+8 image rows
+//     stream through and every row is applied to the 8 candidates that
+//     overlap it. Candidate k lives in accumulator k & 7; with the row loop
+//     unrolled the slots are register names, so a row costs 4 shared loads and
+//     32 subtract/FMA pairs per lane. A finished candidate's two half sums meet
+//     through one shuffle; the sum enters the reference's register top-k, kept
+//     identically by both lanes; the P partial lists merge in shared memory.
 #include "kernels.cuh"
 
 #include <algorithm>
@@ -22,7 +25,7 @@
 namespace nssb {
 namespace {
 
-__device__ __forceinline__ int skew(int col) { return col + (col >> 5); }
+__device__ __forceinline__ int swz(int col) { return col ^ ((col >> 5) & 3); }
 
 __device__ __forceinline__ uint64_t key_of(float d, int x, int y) {
     uint32_t b = __float_as_uint(d);
@@ -49,25 +52,20 @@ struct TopK {
     }
 };
 
-constexpr int kLanes = 32;
+constexpr int kLanes = 32;   // references per CTA
+constexpr int kPitch = 288;  // tile row pitch: >= 31 * 8 + 2 * 9 + 8 columns
 
 template <int R>
 __host__ __device__ constexpr int tile_rows() { return 2 * R + 8; }
 
-int tile_pitch(int step, int R) {
-    const int tw = (kLanes - 1) * step + 2 * R + 8;
-    return ((tw - 1 + ((tw - 1) >> 5)) / 32 + 1) * 32;
-}
-
 template <int R, int K, int P>
-__global__ void __launch_bounds__(kLanes* P, (K <= 7 ? 4 : 3))
-    match8_kernel(const __grid_constant__ MatchBatch mb, int pitch) {
-    constexpr int B = 8;
+__global__ void __launch_bounds__(64 * P, (K <= 7 ? 3 : 2))
+    match8_kernel(const __grid_constant__ MatchBatch mb) {
+    constexpr int B = 8, HB = 4;
     constexpr int NC = 2 * R + 1;            // candidates per window column
     constexpr int TR = tile_rows<R>();
-    constexpr int CPW = (NC + P - 1) / P;    // window columns per warp
+    constexpr int CPW = (NC + P - 1) / P;    // window columns per warp pair
     extern __shared__ float tile[];
-    // this CTA's plane
     int pl = 0;
     {
         int lo = 0, hi = mb.n - 1;
@@ -87,84 +85,102 @@ __global__ void __launch_bounds__(kLanes* P, (K <= 7 ? 4 : 3))
     const int X0 = grid_pos(rx0, W, B, step) - R, Y0 = cy - R;
     const int TW = grid_pos(rx1, W, B, step) + R + B - X0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int r = warp; r < TR; r += P) {
+    for (int r = warp; r < TR; r += 2 * P) {
         const int gy = Y0 + r;
         const bool yok = gy >= 0 && gy < H;
         const float* src = P_.src + (int64_t)(yok ? gy : 0) * P_.stride;
-        float* dst = tile + r * pitch;
-        for (int c = lane; c < TW; c += kLanes) {
+        float* dst = tile + r * kPitch;
+        for (int c = lane; c < TW; c += 32) {
             const int gx = X0 + c;
-            dst[skew(c)] = (yok && gx >= 0 && gx < W) ? __ldg(src + gx) : 0.f;
+            dst[swz(c)] = (yok && gx >= 0 && gx < W) ? __ldg(src + gx) : 0.f;
         }
     }
     __syncthreads();
 
-    const int rx = rx0 + lane;
+    const int rg = warp & 1, part = warp >> 1, half = lane >> 4;
+    const int l = rg * 16 + (lane & 15);
+    const int rx = rx0 + l;
     const bool active = rx < nx;
     const int cx = grid_pos(min(rx, nx - 1), W, B, step);
     const int left = max(cx - R, 0), right = min(cx + R, W - B);
     const int kmin = max(cy - R, 0) - (cy - R), kmax = min(cy + R, H - B) - (cy - R);
-    const int tc0 = cx - R - X0;
+    const int tc0 = cx - R - X0 + HB * half;  // tile column of this half's first block column at dx = -R
 
-    float ref[B * B];
+    float ref[B * HB];
 #pragma unroll
     for (int i = 0; i < B; ++i)
 #pragma unroll
-        for (int j = 0; j < B; ++j) ref[i * B + j] = tile[(R + i) * pitch + skew(tc0 + R + j)];
+        for (int j = 0; j < HB; ++j) ref[i * HB + j] = tile[(R + i) * kPitch + swz(tc0 + R + j)];
 
     TopK<K> topk;
     topk.init();
-    const int d0 = warp * CPW, d1 = min(NC, d0 + CPW);
+    // finished distances of the current column, one slot per candidate row:
+    // an emit stores its sum and marks a bit when it may enter the list; the
+    // insertions run after the column, once per marked candidate
+    float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
+    const uint32_t rows_ok = ((1u << (kmax + 1)) - 1u) & ~((1u << kmin) - 1u);
+    const int d0 = part * CPW, d1 = min(NC, d0 + CPW);
     for (int dxi = d0; dxi < d1; ++dxi) {
         const int x = cx - R + dxi;
         const bool xok = x >= left && x <= right;
-        int col[B];
+        uint32_t pass = 0;
+        const uint32_t worst_hi = uint32_t(topk.k[K - 1] >> 32);
+        int col[HB];
 #pragma unroll
-        for (int j = 0; j < B; ++j) col[j] = skew(tc0 + dxi + j);
+        for (int j = 0; j < HB; ++j) col[j] = swz(tc0 + dxi + j);
         float acc[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) acc[q] = 0.f;
 #pragma unroll
         for (int s = 0; s < NC + B - 1; ++s) {
-            const float* rp = tile + s * pitch;
-            float p[B];
+            float p[HB];
 #pragma unroll
-            for (int j = 0; j < B; ++j) p[j] = rp[col[j]];
+            for (int j = 0; j < HB; ++j) p[j] = tile[s * kPitch + col[j]];
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 const int k = s - i;
                 if (k >= 0 && k < NC) {
 #pragma unroll
-                    for (int j = 0; j < B; ++j) {
-                        const float d = __fsub_rn(ref[i * B + j], p[j]);
+                    for (int j = 0; j < HB; ++j) {
+                        const float d = __fsub_rn(ref[i * HB + j], p[j]);
                         acc[k & 7] = __fmaf_rn(d, d, acc[k & 7]);
                     }
                 }
             }
             const int kd = s - (B - 1);
             if (kd >= 0 && kd < NC) {
-                const float dd = acc[kd & 7];
+                const float part_sum = acc[kd & 7];
                 acc[kd & 7] = 0.f;
-                if (xok && kd >= kmin && kd <= kmax && !(dxi == R && kd == R))
-                    topk.add(key_of(dd, x, cy - R + kd));
+                const float dd = __fadd_rn(part_sum, __shfl_xor_sync(0xffffffffu, part_sum, 16));
+                stash[kd * (64 * P)] = dd;
+                uint32_t b = __float_as_uint(dd);
+                if ((b & 0x7f800000u) == 0x7f800000u) b = 0x7f800000u;
+                pass |= (b <= worst_hi ? 1u : 0u) << kd;
             }
+        }
+        pass &= xok ? rows_ok : 0u;
+        if (dxi == R) pass &= ~(1u << R);
+        while (pass) {
+            const int kd = __ffs(pass) - 1;
+            pass &= pass - 1;
+            topk.add(key_of(stash[kd * (64 * P)], x, cy - R + kd));
         }
     }
     // merge the P partial lists of each reference (exact: keys are a total order)
     if constexpr (P > 1) {
         __syncthreads();
-        uint64_t* keys = reinterpret_cast<uint64_t*>(tile);  // [P][K][32]
-        if (warp > 0) {
+        uint64_t* keys = reinterpret_cast<uint64_t*>(tile);  // [P][K][32 references]
+        if (part > 0 && half == 0) {
 #pragma unroll
-            for (int q = 0; q < K; ++q) keys[(warp * K + q) * kLanes + lane] = topk.k[q];
+            for (int q = 0; q < K; ++q) keys[(part * K + q) * kLanes + l] = topk.k[q];
         }
         __syncthreads();
-        if (warp > 0) return;
+        if (part > 0) return;
         for (int w = 1; w < P; ++w)
 #pragma unroll
-            for (int q = 0; q < K; ++q) topk.add(keys[(w * K + q) * kLanes + lane]);
+            for (int q = 0; q < K; ++q) topk.add(keys[(w * K + q) * kLanes + l]);
     }
-    if (!active) return;
+    if (!active || half != 0) return;
     const int64_t job = (int64_t)ry * nx + rx;
     constexpr int G = K + 1;
     int32_t* op = P_.pos + job * G;
@@ -199,12 +215,12 @@ void launch_rk(MatchBatch& mb, cudaStream_t stream) {
         ctas += ceil_div(p.nx, kLanes) * p.ny;
     }
     if (ctas == 0) return;
-    const int pitch = tile_pitch(mb.step, R);
-    const size_t smem = std::max((size_t)pitch * tile_rows<R>() * sizeof(float),
+    static_assert(31 * 8 + 2 * R + 8 <= kPitch, "tile pitch too small for this range");
+    const size_t smem = std::max((size_t)(kPitch * tile_rows<R>() + (2 * R + 1) * 64 * kParts) * sizeof(float),
                                  (size_t)kParts * K * kLanes * sizeof(uint64_t));
     auto kern = match8_kernel<R, K, kParts>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<ctas, kLanes * kParts, smem, stream>>>(mb, pitch);
+    kern<<<ctas, 64 * kParts, smem, stream>>>(mb);
     NSSB_CUDA(cudaGetLastError());
 }
 

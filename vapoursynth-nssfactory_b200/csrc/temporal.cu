@@ -53,28 +53,37 @@ struct TList {
     }
 };
 
+// SSD in this build's order: left-half and right-half column chains, lo + hi.
 template <int B>
 __device__ float ssd_global(const float* __restrict__ a, int64_t sa, const float* __restrict__ b, int64_t sb) {
-    float acc = 0.f;
+    constexpr int h = B / 2;
+    float lo = 0.f, hi = 0.f;
 #pragma unroll
     for (int i = 0; i < B; ++i)
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const float d = __fsub_rn(__ldg(a + i * sa + j), __ldg(b + i * sb + j));
-            acc = __fmaf_rn(d, d, acc);
+            if (j < h)
+                lo = __fmaf_rn(d, d, lo);
+            else
+                hi = __fmaf_rn(d, d, hi);
         }
-    return acc;
+    return __fadd_rn(lo, hi);
 }
 
 __device__ float ssd_global_rt(const float* __restrict__ a, int64_t sa, const float* __restrict__ b, int64_t sb,
                                int B) {
-    float acc = 0.f;
+    const int h = B / 2;
+    float lo = 0.f, hi = 0.f;
     for (int i = 0; i < B; ++i)
         for (int j = 0; j < B; ++j) {
             const float d = __fsub_rn(__ldg(a + i * sa + j), __ldg(b + i * sb + j));
-            acc = __fmaf_rn(d, d, acc);
+            if (j < h)
+                lo = __fmaf_rn(d, d, lo);
+            else
+                hi = __fmaf_rn(d, d, hi);
         }
-    return acc;
+    return __fadd_rn(lo, hi);
 }
 
 template <int B>
