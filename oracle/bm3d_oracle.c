@@ -33,25 +33,26 @@ float om_noise_effective(float user_sigma) {
 
 /* ---------------------------------------------------------------- distances */
 
-/* The SSD order of this build: the block's left columns [0, B/2) and right
- * columns [B/2, B) each take one FMA chain in row-major order, and the two
- * chains are added once: lo + hi. */
+/* Pairwise sum of n per-column partials: the halves' sums, added. */
+static float column_tree(const float* c, int n) {
+    if (n == 1) return c[0];
+    const int h = n / 2;
+    return column_tree(c, h) + column_tree(c + h, n - h);
+}
+
+/* The SSD order of this build: every block column j takes one FMA chain down
+ * the rows (c_j = fma(d, d, c_j), d = a - b, rows in order), then the
+ * columns are summed pairwise (column_tree: halves first, recursively). */
 float om_ssd(const float* a, ptrdiff_t sa, const float* b, ptrdiff_t sb, int block) {
-    const int h = block >> 1;
-    float lo = 0.f, hi = 0.f;
+    float c[32];
+    for (int j = 0; j < block; ++j) c[j] = 0.f;
     for (int i = 0; i < block; ++i) {
-        for (int j = 0; j < h; ++j) {
+        for (int j = 0; j < block; ++j) {
             const float d = a[i * sa + j] - b[i * sb + j];
-            lo = fmaf(d, d, lo);
+            c[j] = fmaf(d, d, c[j]);
         }
     }
-    for (int i = 0; i < block; ++i) {
-        for (int j = h; j < block; ++j) {
-            const float d = a[i * sa + j] - b[i * sb + j];
-            hi = fmaf(d, d, hi);
-        }
-    }
-    return lo + hi;
+    return column_tree(c, block);
 }
 
 /* The 8-lane tree of SpatialMatch8 (ssd.cpp:207-237): lane j accumulates rows
@@ -145,59 +146,96 @@ int om_grid_pos(int i, int extent, int block, int step) { return imin(i * step, 
  * (buf holds the window rows, each readable for n + 24 + block columns), 24
  * candidates per pass: each keeps its own row-major FMA chain, the lanes are
  * independent, so the compiler's vector form gives om_ssd's bits. */
+#if defined(__AVX2__) && defined(__FMA__)
+static __m256 column_tree8(const __m256* c, int n) {
+    if (n == 1) return c[0];
+    const int h = n / 2;
+    return _mm256_add_ps(column_tree8(c, h), column_tree8(c + h, n - h));
+}
+#endif
+
+#if defined(__AVX2__) && defined(__FMA__)
+/* block 8: the same per-column chains and tree with the accumulators in registers */
+static void ssd_span8(const float* refblk, const float* buf, ptrdiff_t bstride, int n, int nrows, float* out,
+                      int ostride) {
+    for (int q = 0; q < nrows; ++q) {
+        for (int c0 = 0; c0 < n; c0 += 8) {
+            __m256 a0 = _mm256_setzero_ps(), a1 = a0, a2 = a0, a3 = a0, a4 = a0, a5 = a0, a6 = a0, a7 = a0;
+            for (int i = 0; i < 8; ++i) {
+                const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0;
+                const float* r = refblk + i * 8;
+#define NSSB_COL(k, acc)                                                                            \
+    {                                                                                               \
+        const __m256 d = _mm256_sub_ps(_mm256_set1_ps(r[k]), _mm256_loadu_ps(row + k));            \
+        acc = _mm256_fmadd_ps(d, d, acc);                                                           \
+    }
+                NSSB_COL(0, a0) NSSB_COL(1, a1) NSSB_COL(2, a2) NSSB_COL(3, a3)
+                NSSB_COL(4, a4) NSSB_COL(5, a5) NSSB_COL(6, a6) NSSB_COL(7, a7)
+#undef NSSB_COL
+            }
+            const __m256 t = _mm256_add_ps(_mm256_add_ps(_mm256_add_ps(a0, a1), _mm256_add_ps(a2, a3)),
+                                           _mm256_add_ps(_mm256_add_ps(a4, a5), _mm256_add_ps(a6, a7)));
+            float tree[8];
+            _mm256_storeu_ps(tree, t);
+            const int mm = n - c0 < 8 ? n - c0 : 8;
+            for (int l = 0; l < mm; ++l) out[q * ostride + c0 + l] = tree[l];
+        }
+    }
+}
+#endif
+
 static void ssd_span(const float* refblk, int block, const float* buf, ptrdiff_t bstride, int n, int nrows,
                      float* out, int ostride) {
-    /* nrows (<= 2) candidate rows x n candidates; candidate row q starts at
-     * buffer row q. Left and right half-column chains as in om_ssd. */
-    const int h = block >> 1;
-    for (int c0 = 0; c0 < n; c0 += 24) {
-        float lo[2][24], hi[2][24];
+    /* nrows (<= 2) candidate rows x n candidates (8 per vector lane group);
+     * candidate row q starts at buffer row q. Per-column chains and the
+     * column tree as in om_ssd. */
 #if defined(__AVX2__) && defined(__FMA__)
-        /* vfmadd is the exactly rounded fma: the same bits as fmaf */
-        __m256 a[2][3], b[2][3];
-        for (int q = 0; q < 2; ++q)
-            for (int v = 0; v < 3; ++v) a[q][v] = b[q][v] = _mm256_setzero_ps();
-        for (int i = 0; i < block; ++i) {
-            for (int j = 0; j < block; ++j) {
-                const __m256 r = _mm256_set1_ps(refblk[i * block + j]);
-                for (int q = 0; q < 2; ++q) {
-                    const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
-                    for (int v = 0; v < 3; ++v) {
-                        const __m256 d = _mm256_sub_ps(r, _mm256_loadu_ps(row + 8 * v));
-                        if (j < h)
-                            a[q][v] = _mm256_fmadd_ps(d, d, a[q][v]);
-                        else
-                            b[q][v] = _mm256_fmadd_ps(d, d, b[q][v]);
-                    }
+    if (block == 8) {
+        ssd_span8(refblk, buf, bstride, n, nrows, out, ostride);
+        return;
+    }
+#endif
+    for (int q = 0; q < nrows; ++q) {
+        for (int c0 = 0; c0 < n; c0 += 8) {
+            float col[32][8];
+#if defined(__AVX2__) && defined(__FMA__)
+            /* vfmadd is the exactly rounded fma: the same bits as fmaf */
+            __m256 acc[32];
+            for (int j = 0; j < block; ++j) acc[j] = _mm256_setzero_ps();
+            for (int i = 0; i < block; ++i) {
+                const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0;
+                for (int j = 0; j < block; ++j) {
+                    const __m256 d = _mm256_sub_ps(_mm256_set1_ps(refblk[i * block + j]), _mm256_loadu_ps(row + j));
+                    acc[j] = _mm256_fmadd_ps(d, d, acc[j]);
                 }
             }
-        }
-        for (int q = 0; q < 2; ++q)
-            for (int v = 0; v < 3; ++v) {
-                _mm256_storeu_ps(lo[q] + 8 * v, a[q][v]);
-                _mm256_storeu_ps(hi[q] + 8 * v, b[q][v]);
-            }
+            float tree[8];
+            _mm256_storeu_ps(tree, column_tree8(acc, block));
+            const int mm = n - c0 < 8 ? n - c0 : 8;
+            for (int l = 0; l < mm; ++l) out[q * ostride + c0 + l] = tree[l];
+            continue;
+            (void)col;
 #else
-        for (int q = 0; q < 2; ++q)
-            for (int c = 0; c < 24; ++c) lo[q][c] = hi[q][c] = 0.f;
-        for (int i = 0; i < block; ++i)
-            for (int j = 0; j < block; ++j) {
-                const float r = refblk[i * block + j];
-                for (int q = 0; q < 2; ++q) {
-                    const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0 + j;
-                    for (int c = 0; c < 24; ++c) {
-                        const float d = r - row[c];
-                        if (j < h)
-                            lo[q][c] = fmaf(d, d, lo[q][c]);
-                        else
-                            hi[q][c] = fmaf(d, d, hi[q][c]);
+            for (int j = 0; j < block; ++j)
+                for (int l = 0; l < 8; ++l) col[j][l] = 0.f;
+            for (int i = 0; i < block; ++i) {
+                const float* row = buf + (ptrdiff_t)(i + q) * bstride + c0;
+                for (int j = 0; j < block; ++j) {
+                    const float r = refblk[i * block + j];
+                    for (int l = 0; l < 8; ++l) {
+                        const float d = r - row[j + l];
+                        col[j][l] = fmaf(d, d, col[j][l]);
                     }
                 }
             }
 #endif
-        const int m = n - c0 < 24 ? n - c0 : 24;
-        for (int q = 0; q < nrows; ++q)
-            for (int c = 0; c < m; ++c) out[q * ostride + c0 + c] = lo[q][c] + hi[q][c];
+            const int m = n - c0 < 8 ? n - c0 : 8;
+            for (int l = 0; l < m; ++l) {
+                float c[32];
+                for (int j = 0; j < block; ++j) c[j] = col[j][l];
+                out[q * ostride + c0 + l] = column_tree(c, block);
+            }
+        }
     }
 }
 

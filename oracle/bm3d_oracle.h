@@ -20,9 +20,9 @@
  *   - temporal slot mapping                                src/frontend/temporal.hpp:11-36
  *   - noise profile sigma_eff = sigma/255*0.75             include/nss/contracts.hpp:19-30
  *
- * Summation order of the SSD: per candidate, the block's left columns
- * [0, B/2) and right columns [B/2, B) each take one FMA chain in row-major
- * order (acc = fma(d, d, acc), d = a - b), then lo + hi. The reference's SIMD
+ * Summation order of the SSD: per candidate, every block column takes one
+ * FMA chain down the rows (c_j = fma(d, d, c_j), d = a - b), then the
+ * columns are added pairwise (halves first, recursively). The reference's SIMD
  * trees are Highway-target dependent; this order is the one the CUDA
  * matcher also uses, so oracle and device distances are bit-identical and
  * groups agree exactly (om_ssd_lanes8 restates the reference's 8-lane AVX2

@@ -43,4 +43,15 @@ __host__ __device__ inline int32_t pack_pos(int x, int y) { return static_cast<i
 __host__ __device__ inline int pos_x(int32_t p) { return static_cast<int>(uint32_t(p) & 0xffffu); }
 __host__ __device__ inline int pos_y(int32_t p) { return static_cast<int>(uint32_t(p) >> 16); }
 
+// The SSD order of this build: one FMA chain per block column down the
+// rows, then the columns added pairwise (halves first, recursively).
+template <int N>
+__device__ __forceinline__ float column_tree(const float* c) {
+    if constexpr (N == 1) {
+        return c[0];
+    } else {
+        return __fadd_rn(column_tree<N / 2>(c), column_tree<N - N / 2>(c + N / 2));
+    }
+}
+
 }  // namespace nssb

@@ -4,10 +4,10 @@
 // for every reference of the raster grid (last row/column clamped to W-B/H-B)
 // the group is the reference itself, then the group-1 smallest SSDs of the
 // other positions of the clamped (2R+1)^2 window, ordered by distance, then y,
-// then x; non-finite distances after every finite one. The SSD order: the
-// block's left columns [0, B/2) and right columns [B/2, B) each take one FMA
-// chain in row-major order, then lo + hi -- the order of the CPU oracle, so
-// device and oracle distances are bit-identical.
+// then x; non-finite distances after every finite one. The SSD order: one
+// FMA chain per block column down the rows, then the columns added pairwise
+// (column_tree) -- the order of the CPU oracle, so device and oracle
+// distances are bit-identical.
 //
 // Layout: one thread per reference; a CTA covers TX x TY references and stages
 // the union of their windows in shared memory once. Keys are 64-bit
@@ -101,31 +101,26 @@ __device__ void match_one(const float* __restrict__ tile, int tp, int x0, int y0
         for (int x = left; x <= right; ++x) {
             if (x == cx && y == cy) continue;
             const float* cb = rowbase + x;
-            constexpr int h = B / 2;
-            float lo = 0.f, hi = 0.f;
+            float c[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j) c[j] = 0.f;
             if constexpr (kRegs) {
 #pragma unroll
                 for (int i = 0; i < B; ++i)
 #pragma unroll
                     for (int j = 0; j < B; ++j) {
                         const float d = __fsub_rn(ref[i * B + j], cb[i * tp + j]);
-                        if (j < h)
-                            lo = __fmaf_rn(d, d, lo);
-                        else
-                            hi = __fmaf_rn(d, d, hi);
+                        c[j] = __fmaf_rn(d, d, c[j]);
                     }
             } else {
                 for (int i = 0; i < B; ++i)
-#pragma unroll 4
+#pragma unroll
                     for (int j = 0; j < B; ++j) {
                         const float d = __fsub_rn(rb[i * tp + j], cb[i * tp + j]);
-                        if (j < h)
-                            lo = __fmaf_rn(d, d, lo);
-                        else
-                            hi = __fmaf_rn(d, d, hi);
+                        c[j] = __fmaf_rn(d, d, c[j]);
                     }
             }
-            topk.add(match_key(__fadd_rn(lo, hi), x, y));
+            topk.add(match_key(column_tree<B>(c), x, y));
         }
     }
 }

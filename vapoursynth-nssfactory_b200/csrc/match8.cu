@@ -1,9 +1,9 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
-// keys dist << 32 | y << 16 | x, and this build's SSD order: left columns
-// 0-3 and right columns 4-7 each one FMA chain in row-major order, then
-// lo + hi); only the schedule differs:
+// keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
+// block column down the rows, then ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7)));
+// only the schedule differs:
 //   - a CTA is 32 consecutive references of one grid row of one plane of a
 //     batch. Two lanes serve each reference, one per column half, each with
 //     its 8x4 half block in 32 registers; a warp is 16 references x 2 halves
@@ -14,10 +14,12 @@
 //   - a lane walks its window columns one by one: the column's 2R+8 image rows
 //     stream through and every row is applied to the 8 candidates that
 //     overlap it. Candidate k lives in accumulator k & 7; with the row loop
-//     unrolled the slots are register names, so a row costs 4 shared loads and
-//     32 subtract/FMA pairs per lane. A finished candidate's two half sums meet
-//     through one shuffle; the sum enters the reference's register top-k, kept
-//     identically by both lanes; the P partial lists merge in shared memory.
+//     unrolled the slots are register names. The packed FP32 FMA of sm_100
+//     (__ffma2_rn) carries two block columns per instruction, so a row costs 4
+//     shared loads and 32 packed operations per lane. A finished candidate's
+//     two half sums meet through one shuffle; the sum enters the reference's
+//     register top-k, kept identically by both lanes; the P partial lists
+//     merge in shared memory.
 #include "kernels.cuh"
 
 #include <algorithm>
@@ -59,7 +61,7 @@ template <int R>
 __host__ __device__ constexpr int tile_rows() { return 2 * R + 8; }
 
 template <int R, int K, int P>
-__global__ void __launch_bounds__(64 * P, (K <= 7 ? 3 : 2))
+__global__ void __launch_bounds__(64 * P, (K <= 7 ? 4 : 3))
     match8_kernel(const __grid_constant__ MatchBatch mb) {
     constexpr int B = 8, HB = 4;
     constexpr int NC = 2 * R + 1;            // candidates per window column
@@ -106,11 +108,14 @@ __global__ void __launch_bounds__(64 * P, (K <= 7 ? 3 : 2))
     const int kmin = max(cy - R, 0) - (cy - R), kmax = min(cy + R, H - B) - (cy - R);
     const int tc0 = cx - R - X0 + HB * half;  // tile column of this half's first block column at dx = -R
 
-    float ref[B * HB];
+    // this half's 8x4 reference block as column pairs (c, c+1) of each row
+    float2 ref[B][2];
 #pragma unroll
     for (int i = 0; i < B; ++i)
 #pragma unroll
-        for (int j = 0; j < HB; ++j) ref[i * HB + j] = tile[(R + i) * kPitch + swz(tc0 + R + j)];
+        for (int h = 0; h < 2; ++h)
+            ref[i][h] = make_float2(tile[(R + i) * kPitch + swz(tc0 + R + 2 * h)],
+                                    tile[(R + i) * kPitch + swz(tc0 + R + 2 * h + 1)]);
 
     TopK<K> topk;
     topk.init();
@@ -119,43 +124,50 @@ __global__ void __launch_bounds__(64 * P, (K <= 7 ? 3 : 2))
     // insertions run after the column, once per marked candidate
     float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
     const uint32_t rows_ok = ((1u << (kmax + 1)) - 1u) & ~((1u << kmin) - 1u);
+    const float2 neg1 = make_float2(-1.f, -1.f);
+    // this part's columns, walked outwards from the window centre so the
+    // closest candidates (usually the best) fill the list first
     const int d0 = part * CPW, d1 = min(NC, d0 + CPW);
-    for (int dxi = d0; dxi < d1; ++dxi) {
+    const bool down = d1 - 1 <= R;
+    for (int m = 0; m < d1 - d0; ++m) {
+        const int dxi = down ? d1 - 1 - m : d0 + m;
         const int x = cx - R + dxi;
         const bool xok = x >= left && x <= right;
         uint32_t pass = 0;
-        const uint32_t worst_hi = uint32_t(topk.k[K - 1] >> 32);
+        // a candidate may enter unless it is farther than the current worst
+        // (NaN never compares greater: non-finite sums always take the exact path)
+        const float worst = __uint_as_float(uint32_t(topk.k[K - 1] >> 32));
         int col[HB];
 #pragma unroll
         for (int j = 0; j < HB; ++j) col[j] = swz(tc0 + dxi + j);
-        float acc[8];
+        // per-column chains, two columns per packed FMA: acc[k & 7][h] holds
+        // columns (2h, 2h+1) of this half for candidate k
+        float2 acc[8][2];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+        for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int s = 0; s < NC + B - 1; ++s) {
-            float p[HB];
-#pragma unroll
-            for (int j = 0; j < HB; ++j) p[j] = tile[s * kPitch + col[j]];
+            const float2 p01 = make_float2(tile[s * kPitch + col[0]], tile[s * kPitch + col[1]]);
+            const float2 p23 = make_float2(tile[s * kPitch + col[2]], tile[s * kPitch + col[3]]);
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 const int k = s - i;
                 if (k >= 0 && k < NC) {
-#pragma unroll
-                    for (int j = 0; j < HB; ++j) {
-                        const float d = __fsub_rn(ref[i * HB + j], p[j]);
-                        acc[k & 7] = __fmaf_rn(d, d, acc[k & 7]);
-                    }
+                    // r - p exactly as fma(p, -1, r), then the square added
+                    const float2 d01 = __ffma2_rn(p01, neg1, ref[i][0]);
+                    const float2 d23 = __ffma2_rn(p23, neg1, ref[i][1]);
+                    acc[k & 7][0] = __ffma2_rn(d01, d01, acc[k & 7][0]);
+                    acc[k & 7][1] = __ffma2_rn(d23, d23, acc[k & 7][1]);
                 }
             }
             const int kd = s - (B - 1);
             if (kd >= 0 && kd < NC) {
-                const float part_sum = acc[kd & 7];
-                acc[kd & 7] = 0.f;
-                const float dd = __fadd_rn(part_sum, __shfl_xor_sync(0xffffffffu, part_sum, 16));
+                const float2 a = acc[kd & 7][0], b = acc[kd & 7][1];
+                acc[kd & 7][0] = acc[kd & 7][1] = make_float2(0.f, 0.f);
+                const float half_sum = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
+                const float dd = __fadd_rn(half_sum, __shfl_xor_sync(0xffffffffu, half_sum, 16));
                 stash[kd * (64 * P)] = dd;
-                uint32_t b = __float_as_uint(dd);
-                if ((b & 0x7f800000u) == 0x7f800000u) b = 0x7f800000u;
-                pass |= (b <= worst_hi ? 1u : 0u) << kd;
+                pass |= (dd > worst ? 0u : 1u) << kd;
             }
         }
         pass &= xok ? rows_ok : 0u;
@@ -202,7 +214,7 @@ __global__ void __launch_bounds__(64 * P, (K <= 7 ? 3 : 2))
     P_.count[job] = 1 + n;
 }
 
-constexpr int kParts = 4;
+constexpr int kParts = 2;
 
 template <int R, int K>
 void launch_rk(MatchBatch& mb, cudaStream_t stream) {

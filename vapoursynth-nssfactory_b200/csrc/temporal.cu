@@ -53,37 +53,33 @@ struct TList {
     }
 };
 
-// SSD in this build's order: left-half and right-half column chains, lo + hi.
+// SSD in this build's order: per-column FMA chains down the rows, column_tree.
 template <int B>
 __device__ float ssd_global(const float* __restrict__ a, int64_t sa, const float* __restrict__ b, int64_t sb) {
-    constexpr int h = B / 2;
-    float lo = 0.f, hi = 0.f;
+    float c[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) c[j] = 0.f;
 #pragma unroll
     for (int i = 0; i < B; ++i)
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const float d = __fsub_rn(__ldg(a + i * sa + j), __ldg(b + i * sb + j));
-            if (j < h)
-                lo = __fmaf_rn(d, d, lo);
-            else
-                hi = __fmaf_rn(d, d, hi);
+            c[j] = __fmaf_rn(d, d, c[j]);
         }
-    return __fadd_rn(lo, hi);
+    return column_tree<B>(c);
 }
 
 __device__ float ssd_global_rt(const float* __restrict__ a, int64_t sa, const float* __restrict__ b, int64_t sb,
                                int B) {
-    const int h = B / 2;
-    float lo = 0.f, hi = 0.f;
-    for (int i = 0; i < B; ++i)
-        for (int j = 0; j < B; ++j) {
-            const float d = __fsub_rn(__ldg(a + i * sa + j), __ldg(b + i * sb + j));
-            if (j < h)
-                lo = __fmaf_rn(d, d, lo);
-            else
-                hi = __fmaf_rn(d, d, hi);
-        }
-    return __fadd_rn(lo, hi);
+    switch (B) {
+        case 1: return ssd_global<1>(a, sa, b, sb);
+        case 2: return ssd_global<2>(a, sa, b, sb);
+        case 4: return ssd_global<4>(a, sa, b, sb);
+        case 8: return ssd_global<8>(a, sa, b, sb);
+        case 12: return ssd_global<12>(a, sa, b, sb);
+        case 16: return ssd_global<16>(a, sa, b, sb);
+        default: return ssd_global<32>(a, sa, b, sb);
+    }
 }
 
 template <int B>
