@@ -153,6 +153,24 @@ int nssb_match_temporal(const float* const* planes, const int64_t* strides, int 
 int nssb_bm3d_plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int width, int height,
                           float sigma, int block, int group, int step, int bm_range, void* stream);
 
+/* The stage above without allocating anything. No counterpart in the
+ * reference: it is for callers that cannot allocate device memory while they
+ * run -- hosts whose device memory is owned and budgeted by their own pool
+ * (a frame pool sized at start-up), or latency-critical loops where
+ * cudaMalloc/cudaFree would block or synchronise the device. Scratch comes
+ * from one file-scope device array of about 37 MiB that every GPU loading the
+ * library keeps until exit; planes up to 2 MiPx (stride x height <= 2097152),
+ * 262144 references and 1048576 match entries (references x group) are
+ * accepted, larger ones rejected with NSSB_ERR_STATE. Shapes whose group
+ * cube needs global scratch (block 32 with groups of 32 or more, Wiener
+ * block 16 with 64, ...) are rejected too. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress); make it before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race,
+ * so serialise them; each call clears the sums it uses. */
+int nssb_bm3d_plane_stage_noalloc(const float* src, const float* ref, float* dst, int64_t stride, int width,
+                                  int height, float sigma, int block, int group, int step, int bm_range,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -199,4 +199,21 @@ int nssb_bm3d_plane_stage(const float* src, const float* ref, float* dst, int64_
     });
 }
 
+int nssb_bm3d_plane_stage_noalloc(const float* src, const float* ref, float* dst, int64_t stride, int width,
+                                  int height, float sigma, int block, int group, int step, int bm_range,
+                                  void* stream) {
+    return guarded([&] {
+        if (!src || !dst || width < block || height < block || block < 1 || step < 1 || step > block ||
+            group < 1 || group > nssb::kMaxGroup || bm_range < 0 || bm_range > nssb::kMaxRange || stride < width)
+            throw std::invalid_argument("nss_cuda: invalid stage arguments");
+        nssb::StageParams sp;
+        sp.sigma = sigma;
+        sp.block = block;
+        sp.group = group;
+        sp.step = step;
+        sp.bm_range = bm_range;
+        nssb::plane_stage_noalloc(src, ref, dst, stride, width, height, sp, static_cast<cudaStream_t>(stream));
+    });
+}
+
 }  // extern "C"

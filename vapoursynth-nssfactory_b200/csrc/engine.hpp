@@ -119,6 +119,11 @@ private:
     std::unique_ptr<Plan> plan_;
 };
 
+// The one-plane stage without any allocation (noalloc.cu): scratch comes from
+// a file-scope device array of fixed size; sizes beyond it are rejected.
+void plane_stage_noalloc(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,
+                         const StageParams& sp, cudaStream_t stream);
+
 // Device memory helpers (cudaMalloc'd, recorded for release).
 void* dev_alloc(size_t bytes);
 void dev_free(void* p);
