@@ -40,8 +40,6 @@ Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg) {
     }
 }
 
-Engine::~Engine() { release(); }
-
 void Engine::release() {
     for (auto& e : event_pool_) {
         (void)cudaEventDestroy(e.first);
@@ -55,8 +53,6 @@ void Engine::release() {
         stream_ = nullptr;
     }
 }
-
-struct Engine::Plan {};
 
 void Engine::alloc() {
     auto take = [&](size_t bytes) {

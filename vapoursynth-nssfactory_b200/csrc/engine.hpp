@@ -116,7 +116,10 @@ private:
     GroupBatch gbatch_;
     FinishBatch fbatch_;
     std::vector<void*> allocations_;
-    std::unique_ptr<Plan> plan_;
+    struct PlanDeleter {
+        void operator()(Plan* p) const;
+    };
+    std::unique_ptr<Plan, PlanDeleter> plan_;
 };
 
 // The one-plane stage without any allocation (noalloc.cu): scratch comes from
