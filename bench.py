@@ -266,10 +266,10 @@ def our_arm(args):
     achieved = flops_per_launch / (per_launch_ms / 1e3) / 1e12 if per_launch_ms > 0 else 0.0
     fp32_peak = FP32_LANES * 2 * sm_max * 1e6 / 1e12
     traffic = None
-    tfile = ROOT / "profiles" / "match_traffic.txt"
+    tfile = ROOT / "profiles" / "match8_group8_finish_two_stage_yuv420_1080p.md"
     if tfile.exists():
         for line in tfile.read_text().splitlines():
-            if line.startswith("bytes_per_launch_c2="):
+            if line.strip().startswith("bytes_per_launch_c2="):
                 traffic = float(line.split("=", 1)[1])
     out = {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
