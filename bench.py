@@ -7,12 +7,16 @@ half-resolution gradient chroma, Gaussian noise 5/255), two-stage BM3D
 all 30 frames once. The inputs (373 MB) exceed the 126 MB L2, so every frame
 is read cold.
 
-- value: frames/s with frames resident in device memory (get_frame on device
-  planes), device time from CUDA events, max over ranks; N ranks process N
-  independent clips (weak scaling, no collective on the data path).
-- e2e: the same through the public call with pinned host frames: the
-  host->device copy of each frame and the device->host copy of its result
-  are inside the timed region.
+- value: frames/s of the batched form (one nssb_batch_run over the step's 30
+  frames: one launch per kernel and stage, a replayed CUDA graph, autotuned
+  launch shapes) with frames resident in device memory; device time from CUDA
+  events, max over ranks; N ranks process N independent clips (weak scaling,
+  no collective on the data path). forms.plain_fps is the per-frame drop-in
+  (nssb_bm3d_get_frame per frame) on the same frames; the two give the same
+  bits.
+- e2e: the batched call on pinned host frames: the host->device copy of each
+  frame and the device->host copy of its result are inside the timed region
+  (chunks on two streams overlap copies and kernels).
 - roofline: the dominant kernel (exact FP32 matcher), algorithmic flops
   (3 * B^2 per reference-candidate pair) over its event-timed duration,
   against the FP32 SIMT peak (148 SMs x 128 lanes x 2 flops x clock).
@@ -209,39 +213,60 @@ def our_arm(args):
     node_d = nssb.BM3D(nssb.Clip.from_frames(dframes, nssb.YUV, 1, 1), sigma=SIGMA, final=1, device_id=local)
     node_h = nssb.BM3D(nssb.Clip.from_frames(hframes_np, nssb.YUV, 1, 1), sigma=SIGMA, final=1, device_id=local)
 
+    batch = nssb.Batch(device_id=local)
+    reqs_d = [(node_d, n) for n in range(nf)]
+    reqs_h = [(node_h, n) for n in range(nf)]
+
     def barrier():
         if pg is not None:
             pg.barrier()
 
-    def device_step():
+    def plain_step():
         for n in range(nf):
             node_d.get_frame(n, out=dout[n])
 
+    def batched_step():
+        batch.run(reqs_d, outs=dout)
+
     def host_step():
-        for n in range(nf):
-            node_h.get_frame(n, out=hout_np[n])
+        batch.run(reqs_h, outs=hout_np)
 
-    for _ in range(args.warmup):
-        device_step()
-    torch.cuda.synchronize()
-    node_d.stats(True, True)
-
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    def timed(step):
+        """Device time of args.steps steps (CUDA events, barrier + sync on both sides)."""
+        for _ in range(args.warmup):
+            step()
+        barrier()
+        torch.cuda.synchronize()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         for _ in range(args.steps):
-            device_step()
+            step()
         end.record()
         torch.cuda.synchronize()
-    barrier()
-    dev_ms = start.elapsed_time(end)
-    stats = node_d.stats(False, True)
-    clock = clocks.summary()
+        barrier()
+        return start.elapsed_time(end)
 
-    # e2e through host frames
-    for _ in range(max(1, args.warmup // 2)):
+    # plain form: per-frame get_frame (kernel stats for the roofline)
+    plain_ms = timed(plain_step)
+    node_d.stats(True, True)
+    for n in range(nf):
+        node_d.get_frame(n, out=dout[n])
+    torch.cuda.synchronize()
+    stats = node_d.stats(False, True)
+    with ClockSampler(local) as clocks:
+        dev_ms = timed(batched_step)
+    clock = clocks.summary()
+    binfo = batch.info()
+    # the batched form's outputs equal the plain form's, bit for bit
+    check_out = [tuple(torch.empty_like(p) for p in f) for f in dframes[:2]]
+    for n in range(2):
+        node_d.get_frame(n, out=check_out[n])
+    batched_step()
+    torch.cuda.synchronize()
+    identical = all(torch.equal(a, b) for n in range(2) for a, b in zip(check_out[n], dout[n]))
+
+    # e2e: the batched call on pinned host frames, copies inside the timed region
+    for _ in range(max(1, args.warmup)):
         host_step()
     barrier()
     torch.cuda.synchronize()
@@ -251,13 +276,15 @@ def our_arm(args):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     barrier()
+    hinfo = batch.info()
 
     if pg is not None:
-        t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=dev)
+        t = torch.tensor([dev_ms, e2e_s, plain_ms], dtype=torch.float64, device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms, e2e_s = float(t[0]), float(t[1])
+        dev_ms, e2e_s, plain_ms = float(t[0]), float(t[1]), float(t[2])
 
     value = world * nf * args.steps / (dev_ms / 1e3)
+    plain_value = world * nf * args.steps / (plain_ms / 1e3)
     e2e = world * nf * args.steps / e2e_s
     hbm, sm_max, peak_kind = peaks()
     launches = stats.match_launches
@@ -277,8 +304,13 @@ def our_arm(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, 30 distinct frames per rank)",
         "config": {"workload": "two-stage BM3D (final=1), YUV420PS 1920x1080, sigma 5, radius 0, default "
                                "block 8 / step 8 / bm_range 9 / group 8", "frames_per_step": nf,
-                   "form": "plain (per-frame get_frame, device-resident frames)",
+                   "form": "batched (one nssb_batch_run over the step's frames, device-resident, graph replay)",
                    "l2": "inputs larger than L2 (30 x 12.4 MB per rank)", "parallelism": f"replicas x{world}"},
+        "forms": {"plain_fps": plain_value, "batched_fps": value, "batched_over_plain": value / plain_value,
+                  "batched_equals_plain_bitwise": bool(identical),
+                  "batched_shape": {"match_parts": binfo.match_parts, "match_persistent": binfo.match_persistent,
+                                    "group_warps": binfo.group_warps, "group_ctas_per_sm": binfo.group_ctas_per_sm},
+                  "batched_kernels_per_step": int(binfo.kernel_launches), "e2e_chunks": int(hinfo.chunks)},
         "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": nf * PLANE_BYTES,
                 "d2h_bytes_per_step": nf * PLANE_BYTES},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
@@ -286,9 +318,9 @@ def our_arm(args):
                      "kernel": "spatial_match_kernel (exact FP32 SSD + top-k)",
                      "peak_kind": f"derived: 148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz ({peak_kind} max clock)",
                      "avg_launch_ms": per_launch_ms, "flops_per_launch": flops_per_launch},
-        "gpu_launches": int(stats.launches),
-        "kernel_ms_per_step": {"match": stats.match_ms / args.steps, "group": stats.group_ms / args.steps,
-                               "finish": stats.finish_ms / args.steps},
+        "gpu_launches": int(binfo.kernel_launches) * args.steps,
+        "kernel_ms_per_step": {"match": stats.match_ms, "group": stats.group_ms, "finish": stats.finish_ms,
+                               "note": "plain form, one pass over the step's frames"},
         "clocks": clock,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -300,6 +332,7 @@ def our_arm(args):
         out["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                                "sample": f"{done} of the workload's frames, frame-parallel, {el:.1f} s; CPU "
                                          "restatement of nss.BM3D (oracle/), not the reference binary"}
+    batch.close()
     node_d.close()
     node_h.close()
     if rank == 0:

@@ -171,6 +171,51 @@ int nssb_bm3d_plane_stage_noalloc(const float* src, const float* ref, float* dst
                                   int height, float sigma, int block, int group, int step, int bm_range,
                                   void* stream);
 
+/* ---- batched form ----
+ * Many output frames of radius-0 filter instances -- different clips,
+ * resolutions, formats, sigmas and stage arguments -- rendered in one pass:
+ * each stage is one launch per kernel and block shape over every plane of
+ * every frame, the two-stage pipeline is captured once per batch layout as
+ * a CUDA graph and replayed, and the kernels' launch shapes are chosen by
+ * timing the candidates on the first batch of each layout. The output of
+ * every frame is bit-identical to nssb_bm3d_get_frame of the same node.
+ * No single reference counterpart: the reference renders frame by frame
+ * through VapourSynth's frame threads (src/cuda/bm3d/filter_bm3d.cpp:73-494,
+ * the getFrame of src/cuda/common/group_driver.cpp:1803). */
+typedef struct nssb_batch nssb_batch;
+typedef struct nssb_batch_item {
+    nssb_bm3d* node;        /* a radius-0 filter instance on the batch's device */
+    const nssb_frame* clip; /* the output frame's input planes */
+    const nssb_frame* ref;  /* its ref-clip frame when the node has one, else NULL */
+    int memory;             /* NSSB_MEM_HOST / NSSB_MEM_DEVICE for clip, ref and out */
+    nssb_frame_out* out;
+} nssb_batch_item;
+typedef struct nssb_batch_info {
+    int match_parts, match_persistent;  /* matcher shape in use */
+    int group_warps, group_ctas_per_sm; /* group-filter shape in use */
+    int graphs;                         /* 1: runs replay a captured graph */
+    int64_t runs, frames;               /* batches and frames rendered */
+    int64_t kernel_launches;            /* kernels per run of the current layout */
+    int64_t graph_builds, tunings;
+    int chunks;                         /* chunks of the last run */
+    double last_run_ms;                 /* device time of the last run, copies included (CUDA events) */
+    size_t arena_bytes;                 /* device memory of the kept layouts */
+} nssb_batch_info;
+/* args (ints): "autotune" (default 1), "graph" (default 1), "chunk_frames"
+ * (frames per chunk; default 0: one chunk when every item is on the device,
+ * else up to four equal chunks on two streams so that host copies overlap
+ * the kernels), and the shapes
+ * used when autotune is 0: "match_parts" (1, 2, 4; default 2),
+ * "match_persistent" (0/1; default 0), "group_warps" (2, 4, 8; default 4),
+ * "group_ctas_per_sm" (1..64; default 16). */
+int nssb_batch_create(int device_id, const nssb_arg* args, int nargs, nssb_batch** out);
+/* Renders items[0..n); returns when every output is written. Every node
+ * must have radius 0 and live on the batch's device. Host planes should be
+ * page-locked for the copies to overlap. */
+int nssb_batch_run(nssb_batch* b, const nssb_batch_item* items, int n);
+int nssb_batch_get_info(nssb_batch* b, nssb_batch_info* out);
+void nssb_batch_free(nssb_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

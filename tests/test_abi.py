@@ -47,3 +47,18 @@ def test_create_without_device_is_a_creation_error(nssb):
         assert str(e).startswith("nss_cuda.BM3D: no CUDA device available")
     else:
         raise AssertionError("creation without a device must fail")
+
+
+def test_batch_create_checks_arguments_then_device(nssb):
+    import pytest
+    import torch
+
+    with pytest.raises(nssb.Error, match="unknown argument bogus"):
+        nssb.Batch(bogus=1)
+    with pytest.raises(nssb.Error, match="match_parts must be 1, 2 or 4"):
+        nssb.Batch(autotune=False, match_parts=3)
+    with pytest.raises(nssb.Error, match="group_warps must be 2, 4 or 8"):
+        nssb.Batch(autotune=False, group_warps=16)
+    if not torch.cuda.is_available():
+        with pytest.raises(nssb.Error, match="nss_batch: no CUDA device available"):
+            nssb.Batch()

@@ -93,6 +93,21 @@ class KernelStats(C.Structure):
 _lib = None
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("node", C.c_void_p), ("clip", C.POINTER(Frame)), ("ref", C.POINTER(Frame)), ("memory", C.c_int),
+                ("out", C.POINTER(FrameOut))]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("match_parts", C.c_int), ("match_persistent", C.c_int), ("group_warps", C.c_int),
+                ("group_ctas_per_sm", C.c_int), ("graphs", C.c_int), ("runs", C.c_int64), ("frames", C.c_int64),
+                ("kernel_launches", C.c_int64), ("graph_builds", C.c_int64), ("tunings", C.c_int64),
+                ("chunks", C.c_int), ("last_run_ms", C.c_double), ("arena_bytes", C.c_size_t)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 def lib():
     """The loaded library; raises if it is missing (no fallback)."""
     global _lib
@@ -123,6 +138,11 @@ def lib():
                                             C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.nssb_bm3d_plane_stage_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                                     C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.nssb_batch_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
+        L.nssb_batch_run.argtypes = [C.c_void_p, C.POINTER(BatchItem), C.c_int]
+        L.nssb_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]
+        L.nssb_batch_free.argtypes = [C.c_void_p]
+        L.nssb_batch_free.restype = None
         _lib = L
     return _lib
 
@@ -288,6 +308,76 @@ class Node:
         check(lib().nssb_bm3d_get_frame(self.handle, n, src, ref, first, last - first + 1,
                                         MEM_DEVICE if device else MEM_HOST, C.byref(fo)))
         return out
+
+
+def _frame_struct(planes, cls=Frame):
+    f = cls()
+    for p, plane in enumerate(planes):
+        ptr, stride = _plane_ptr(plane)
+        f.planes[p] = ptr
+        f.strides[p] = stride
+    return f
+
+
+class Batch:
+    """The batched form: many radius-0 output frames (of any nodes) per call.
+
+    ``run([(node, n), ...])`` renders frame n of each node and returns the
+    output planes in order (numpy, or CUDA tensors for device-resident clips);
+    every output is bit-identical to ``node.get_frame(n)``.
+    """
+
+    def __init__(self, device_id: int = 0, autotune: bool = True, graph: bool = True, **shape):
+        vals = {"autotune": int(autotune), "graph": int(graph), **{k: int(v) for k, v in shape.items()}}
+        arrs = [(C.c_int64 * 1)(v) for v in vals.values()]
+        args = (Arg * len(vals))(*[Arg(k.encode(), ARG_INT, 1, a, None, None) for k, a in zip(vals, arrs)])
+        h = C.c_void_p()
+        check(lib().nssb_batch_create(device_id, args, len(vals), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().nssb_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self) -> BatchInfo:
+        inf = BatchInfo()
+        check(lib().nssb_batch_get_info(self.handle, C.byref(inf)))
+        return inf
+
+    def run(self, requests, outs=None):
+        n = len(requests)
+        items = (BatchItem * n)()
+        keep = []
+        results = []
+        for i, (node, fn) in enumerate(requests):
+            device = node.clip.device
+            src = _frame_struct(node.clip.frames[fn])
+            ref = _frame_struct(node.ref.frames[fn]) if node.ref is not None else None
+            if outs is not None:
+                out = outs[i]
+            else:
+                shapes = [node.vi.plane_shape(p) for p in range(node.vi.planes())]
+                if device:
+                    import torch
+
+                    dev = node.clip.frames[0][0].device
+                    out = tuple(torch.empty(s, dtype=torch.float32, device=dev) for s in shapes)
+                else:
+                    out = tuple(np.empty(s, np.float32) for s in shapes)
+            fo = _frame_struct(out, FrameOut)
+            keep += [src, ref, fo]
+            items[i].node = node.handle
+            items[i].clip = C.pointer(src)
+            items[i].ref = C.pointer(ref) if ref is not None else None
+            items[i].memory = MEM_DEVICE if device else MEM_HOST
+            items[i].out = C.pointer(fo)
+            results.append(out)
+        check(lib().nssb_batch_run(self.handle, items, n))
+        return results
 
 
 def BM3D(clip: Clip, ref: Clip | None = None, **kwargs) -> Node:

@@ -3,15 +3,21 @@
 // boundary, src/frontend/validate.hpp:36-52, src/frontend/ownership.hpp:157-165).
 #include "nss_b200.h"
 
+#include "batch.hpp"
 #include "engine.hpp"
 
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 struct nssb_bm3d {
     std::unique_ptr<nssb::Engine> engine;
+};
+
+struct nssb_batch {
+    std::unique_ptr<nssb::BatchEngine> engine;
 };
 
 namespace {
@@ -44,6 +50,23 @@ int guarded(F&& f) {
     } catch (...) {
         return fail(NSSB_ERR_STATE, "nss: unexpected failure");
     }
+}
+
+// acquire_device (context.cpp:43-60): a creation error, never a render error.
+void acquire_device(int device_id, const char* who) {
+    int count = 0;
+    const cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        throw nssb::ArgumentError(std::string(who) + ": no CUDA device available (" + cudaGetErrorString(e) + ")");
+    }
+    if (device_id < 0 || device_id >= count)
+        throw nssb::ArgumentError(std::string(who) + ": device_id " + std::to_string(device_id) +
+                                  " is out of range (" + std::to_string(count) + " devices)");
+    cudaDeviceProp prop{};
+    NSSB_CUDA(cudaGetDeviceProperties(&prop, device_id));
+    if (prop.major != 10 || prop.minor != 0)
+        throw nssb::ArgumentError(std::string(who) + ": this build runs on sm_100 (B200) devices only");
 }
 
 }  // namespace
@@ -96,21 +119,7 @@ int nssb_bm3d_create(const nssb_video_info* clip, const nssb_video_info* ref, co
     return guarded([&] {
         if (!clip || !out) throw nssb::ArgumentError("nss_cuda.BM3D: clip missing");
         const nssb::Bm3dConfig cfg = nssb::parse_bm3d_call(*clip, ref, args, nargs);
-        // acquire_device (context.cpp:43-60): a creation error, never a render error
-        int count = 0;
-        const cudaError_t e = cudaGetDeviceCount(&count);
-        if (e != cudaSuccess || count == 0) {
-            (void)cudaGetLastError();
-            throw nssb::ArgumentError(std::string("nss_cuda.BM3D: no CUDA device available (") +
-                                      cudaGetErrorString(e) + ")");
-        }
-        if (cfg.device_id >= count)
-            throw nssb::ArgumentError("nss_cuda.BM3D: device_id " + std::to_string(cfg.device_id) +
-                                      " is out of range (" + std::to_string(count) + " devices)");
-        cudaDeviceProp prop{};
-        NSSB_CUDA(cudaGetDeviceProperties(&prop, cfg.device_id));
-        if (prop.major != 10 || prop.minor != 0)
-            throw nssb::ArgumentError("nss_cuda.BM3D: this build runs on sm_100 (B200) devices only");
+        acquire_device(cfg.device_id, "nss_cuda.BM3D");
         auto h = std::make_unique<nssb_bm3d>();
         h->engine = std::make_unique<nssb::Engine>(cfg);
         *out = h.release();
@@ -215,5 +224,65 @@ int nssb_bm3d_plane_stage_noalloc(const float* src, const float* ref, float* dst
         nssb::plane_stage_noalloc(src, ref, dst, stride, width, height, sp, static_cast<cudaStream_t>(stream));
     });
 }
+
+int nssb_batch_create(int device_id, const nssb_arg* args, int nargs, nssb_batch** out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("nssb_batch_create: out missing");
+        nssb::BatchOptions opt;
+        for (int i = 0; i < nargs; ++i) {
+            const nssb_arg& a = args[i];
+            const std::string key = a.key ? a.key : "";
+            int* slot = key == "match_parts"         ? &opt.fixed.match.parts
+                        : key == "match_persistent"  ? &opt.fixed.match.persistent
+                        : key == "group_warps"       ? &opt.fixed.group.warps
+                        : key == "group_ctas_per_sm" ? &opt.fixed.group.ctas_per_sm
+                                                     : nullptr;
+            if (key == "chunk_frames") slot = &opt.chunk_frames;
+            if (key != "autotune" && key != "graph" && !slot)
+                throw nssb::ArgumentError("nss_batch: unknown argument " + key);
+            if (a.type != NSSB_ARG_INT || a.count != 1 || !a.ints)
+                throw nssb::ArgumentError("nss_batch: " + key + " must be one int");
+            const int64_t v = a.ints[0];
+            if (key == "autotune") opt.autotune = v != 0;
+            else if (key == "graph") opt.graphs = v != 0;
+            else *slot = (int)v;
+        }
+        const nssb::LaunchTunes& f = opt.fixed;
+        if (f.match.parts != 1 && f.match.parts != 2 && f.match.parts != 4)
+            throw nssb::ArgumentError("nss_batch: match_parts must be 1, 2 or 4");
+        if (f.group.warps != 2 && f.group.warps != 4 && f.group.warps != 8)
+            throw nssb::ArgumentError("nss_batch: group_warps must be 2, 4 or 8");
+        if (opt.chunk_frames < 0) throw nssb::ArgumentError("nss_batch: chunk_frames must not be negative");
+        if (f.group.ctas_per_sm < 1 || f.group.ctas_per_sm > 64)
+            throw nssb::ArgumentError("nss_batch: group_ctas_per_sm must be in [1, 64]");
+        acquire_device(device_id, "nss_batch");
+        auto h = std::make_unique<nssb_batch>();
+        h->engine = std::make_unique<nssb::BatchEngine>(device_id, opt);
+        *out = h.release();
+    });
+}
+
+int nssb_batch_run(nssb_batch* b, const nssb_batch_item* items, int n) {
+    return guarded([&] {
+        if (!b || (n > 0 && !items) || n < 0) throw std::invalid_argument("nssb_batch_run: invalid arguments");
+        std::vector<nssb::BatchItem> list((size_t)n);
+        for (int i = 0; i < n; ++i) {
+            const nssb_batch_item& it = items[i];
+            if (!it.node) throw std::invalid_argument("nssb_batch_run: item without node");
+            list[i] = nssb::BatchItem{&it.node->engine->config(), it.clip, it.ref, it.memory, it.out};
+        }
+        b->engine->run(list.data(), n);
+    });
+}
+
+int nssb_batch_get_info(nssb_batch* b, nssb_batch_info* out) {
+    return guarded([&] {
+        if (!b || !out) throw std::invalid_argument("nssb_batch_get_info: invalid arguments");
+        b->engine->info(out);
+    });
+}
+
+void nssb_batch_free(nssb_batch* b) { delete b; }
 
 }  // extern "C"

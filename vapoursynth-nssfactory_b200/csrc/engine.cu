@@ -28,7 +28,7 @@ int64_t pitch_of(int w) { return (int64_t)((w + 31) / 32) * 32; }
 
 }  // namespace
 
-Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg) {
+Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg), tables_(new StageTables) {
     device_ = cfg.device_id;
     NSSB_CUDA(cudaSetDevice(device_));
     NSSB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -115,20 +115,21 @@ const float* Engine::device_input(int plane, const nssb_frame* frames, int first
     return d.p;
 }
 
-template <class F>
-void Engine::timed(Kind kind, F&& launch) {
-    if (!timing_) {
-        launch();
-    } else {
+void Engine::clock_begin(Kind) {
+    if (!timing_) return;
+    const size_t i = pending_.size();
+    if (i >= event_pool_.size()) {
+        cudaEvent_t a, b;
+        NSSB_CUDA(cudaEventCreate(&a));
+        NSSB_CUDA(cudaEventCreate(&b));
+        event_pool_.emplace_back(a, b);
+    }
+    NSSB_CUDA(cudaEventRecord(event_pool_[i].first, stream_));
+}
+
+void Engine::clock_end(Kind kind) {
+    if (timing_) {
         const size_t i = pending_.size();
-        if (i >= event_pool_.size()) {
-            cudaEvent_t a, b;
-            NSSB_CUDA(cudaEventCreate(&a));
-            NSSB_CUDA(cudaEventCreate(&b));
-            event_pool_.emplace_back(a, b);
-        }
-        NSSB_CUDA(cudaEventRecord(event_pool_[i].first, stream_));
-        launch();
         NSSB_CUDA(cudaEventRecord(event_pool_[i].second, stream_));
         pending_.emplace_back((int)kind, i);
     }
@@ -153,17 +154,7 @@ void Engine::collect_timing() {
 // Algorithmic work of one matching launch: every reference against every
 // other position of its clamped window, 3 * B^2 flops per pair.
 void Engine::count_match(int w, int h, const StageParams& sp) {
-    auto axis = [&](int extent) {
-        const int n = grid_count(extent, sp.block, sp.step);
-        double sum = 0;
-        for (int i = 0; i < n; ++i) {
-            const int c = grid_pos(i, extent, sp.block, sp.step);
-            sum += std::min(c + sp.bm_range, extent - sp.block) - std::max(c - sp.bm_range, 0) + 1;
-        }
-        return std::make_pair(sum, (double)n);
-    };
-    const auto ax = axis(w), ay = axis(h);
-    const double pairs = ax.first * ay.first - ax.second * ay.second;
+    const double pairs = match_pairs(w, h, sp);
     stats_.match_pairs += pairs;
     stats_.match_flops += pairs * 3.0 * sp.block * sp.block;
 }
@@ -175,121 +166,17 @@ void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
     timing_ = enable_timing != 0;
 }
 
-// One stage over several planes (radius 0): match on ref (Wiener) or src
-// (hard threshold), filter every group, finish. Planes that share a shape go
-// through one launch per kernel; sigma 0 copies the plane.
+// One stage over the planes of a frame (radius 0), one launch per kernel and shape.
 void Engine::run_stage(StageItem* items, int n) {
-    int live[3], nl = 0;
+    StagePlane planes[3];
     for (int i = 0; i < n; ++i) {
         const StageItem& it = items[i];
-        const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
-        if (it.sp->sigma == 0.f) {
-            NSSB_CUDA(cudaMemcpy2DAsync(it.dst, it.dstride * sizeof(float), it.src, it.sstride * sizeof(float),
-                                        w * sizeof(float), h, cudaMemcpyDeviceToDevice, stream_));
-        } else {
-            live[nl++] = i;
-        }
+        planes[i] = StagePlane{it.sp, it.src, it.sstride, it.ref, it.rstride, it.dst, it.dstride,
+                               cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], acc_[it.plane], &scratch_[it.plane],
+                               it.shared_pos, it.shared_count};
     }
-    bool done[3] = {false, false, false};
-    for (int a = 0; a < nl; ++a) {
-        if (done[a]) continue;
-        // the planes of this shape
-        int set[3], ns = 0;
-        const StageItem& first = items[live[a]];
-        for (int b = a; b < nl; ++b) {
-            const StageItem& it = items[live[b]];
-            const StageParams &x = *it.sp, &y = *first.sp;
-            if (!done[b] && x.block == y.block && x.group == y.group && x.step == y.step && x.bm_range == y.bm_range &&
-                (it.ref != nullptr) == (first.ref != nullptr)) {
-                set[ns++] = live[b];
-                done[b] = true;
-            }
-        }
-        const StageParams& sp = *first.sp;
-        const bool wiener = first.ref != nullptr;
-        // matching: batched 8x8 kernel when the shape has it, else the generic one per plane
-        mbatch_.n = 0;
-        mbatch_.step = sp.step;
-        for (int q = 0; q < ns; ++q) {
-            const StageItem& it = items[set[q]];
-            if (it.shared_pos) continue;
-            StageScratch& sc = scratch_[it.plane];
-            mbatch_.p[mbatch_.n++] = MatchPlane{wiener ? it.ref : it.src, wiener ? it.rstride : it.sstride, sc.pos,
-                                                sc.dist, sc.count, cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], 0,
-                                                0, 0};
-            count_match(cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], sp);
-        }
-        if (mbatch_.n > 0) {
-            bool ok = false;
-            if (sp.block == 8) timed(kMatch, [&] { ok = launch_match8_batch(mbatch_, sp.bm_range, sp.group, stream_); });
-            if (!ok) {
-                for (int q = 0; q < mbatch_.n; ++q) {
-                    const MatchPlane& m = mbatch_.p[q];
-                    timed(kMatch, [&] {
-                        launch_match_spatial(m.src, m.stride, m.W, m.H, sp.block, sp.step, sp.bm_range, sp.group,
-                                             m.pos, m.dist, m.count, stream_);
-                    });
-                }
-            }
-        }
-        for (int q = 0; q < ns; ++q) {
-            const AccPlane& ac = acc_[items[set[q]].plane];
-            NSSB_CUDA(cudaMemsetAsync(ac.wsum, 0, (size_t)ac.pitch * cfg_.plane_h[items[set[q]].plane] * 8, stream_));
-        }
-        // group filtering
-        gbatch_.n = 0;
-        gbatch_.total_jobs = 0;
-        for (int q = 0; q < ns; ++q) {
-            const StageItem& it = items[set[q]];
-            const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
-            const int jobs = grid_count(w, sp.block, sp.step) * grid_count(h, sp.block, sp.step);
-            const AccPlane& ac = acc_[it.plane];
-            const StageScratch& sc = scratch_[it.plane];
-            gbatch_.p[gbatch_.n++] = GroupPlane{it.src, it.ref, it.sstride, it.rstride, ac.num, ac.wsum, ac.pitch,
-                                                it.shared_pos ? it.shared_pos : sc.pos,
-                                                it.shared_count ? it.shared_count : sc.count, gbatch_.total_jobs, jobs,
-                                                it.sp->sigma, w, h, 0};
-            gbatch_.total_jobs += jobs;
-        }
-        bool gok = false;
-        if (sp.block == 8)
-            timed(kGroup, [&] {
-                gok = launch_group8_batch(gbatch_, sp.group, wiener, stream_);
-            });
-        if (!gok) {
-            for (int q = 0; q < gbatch_.n; ++q) {
-                const GroupPlane& g = gbatch_.p[q];
-                const StageItem& it = items[set[q]];
-                GroupIO io{};
-                io.src[0] = g.src;
-                io.ref[0] = g.ref;
-                io.stride = g.stride;
-                io.ref_stride = g.ref_stride;
-                io.num[0] = g.num;
-                io.wsum[0] = g.wsum;
-                io.acc_stride = g.acc_stride;
-                const StageScratch& sc = scratch_[it.plane];
-                timed(kGroup, [&] {
-                    launch_group_filter(io, cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], g.pos, nullptr, g.count,
-                                        g.njobs, sp.block, sp.group, g.sigma, wiener, sc.cube, sc.cube_floats,
-                                        stream_);
-                });
-            }
-        }
-        // finish (clears num)
-        fbatch_.n = 0;
-        fbatch_.block = sp.block;
-        fbatch_.total_ctas = 0;
-        for (int q = 0; q < ns; ++q) {
-            const StageItem& it = items[set[q]];
-            const int w = cfg_.plane_w[it.plane], h = cfg_.plane_h[it.plane];
-            const AccPlane& ac = acc_[it.plane];
-            fbatch_.p[fbatch_.n++] = FinishPlane{ac.num, ac.wsum, ac.pitch, it.src, it.sstride, it.dst, it.dstride, w,
-                                                 h, finish_tiles_x(w), fbatch_.total_ctas};
-            fbatch_.total_ctas += finish_tiles(w, h);
-        }
-        timed(kFinish, [&] { launch_finish_batch(fbatch_, stream_); });
-    }
+    Clock clock(this);
+    run_stage_planes(planes, n, stream_, tunes_, clock, *tables_);
 }
 
 void Engine::spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory) {

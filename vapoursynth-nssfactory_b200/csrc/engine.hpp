@@ -8,6 +8,7 @@
 
 #include "kernels.cuh"
 #include "params.hpp"
+#include "stage.hpp"
 
 #include <map>
 #include <memory>
@@ -21,24 +22,6 @@ struct DevPlane {
     float* p = nullptr;
     int64_t pitch = 0;  // elements
     int w = 0, h = 0;
-};
-
-// Fixed-point accumulators of one target frame plane.
-struct AccPlane {
-    long long* num = nullptr;
-    long long* wsum = nullptr;
-    int64_t pitch = 0;
-};
-
-// Scratch of one stage pass: match lists, group cubes.
-struct StageScratch {
-    int32_t* pos = nullptr;
-    int32_t* slot = nullptr;
-    float* dist = nullptr;
-    int32_t* count = nullptr;
-    size_t jobs_cap = 0, group_cap = 0;
-    float* cube = nullptr;
-    size_t cube_floats = 0;
 };
 
 // One plane of one stage of a frame: where it reads, matches and writes.
@@ -75,6 +58,14 @@ public:
     void get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
                    nssb_frame_out* out);
 
+    // Starts a new clip of num_frames frames on this engine's buffers (the
+    // serving form reuses engines): cached window frames and rolling sums are
+    // dropped.
+    void reset_clip(int num_frames);
+    // Device bytes an engine of this configuration allocates (temporal plan
+    // and window caches included; host_frames: frames arrive in host memory).
+    static size_t footprint(const Bm3dConfig& cfg, bool host_frames);
+
     // Kernel accounting (nssb_bm3d_stats).
     void stats(int enable_timing, int reset, nssb_kernel_stats* out);
 
@@ -95,11 +86,25 @@ private:
     void temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
                         nssb_frame_out* out);
 
-    enum Kind { kMatch = 0, kGroup = 1, kFinish = 2 };
+    using Kind = StageClock::Kind;
+    static constexpr Kind kMatch = StageClock::kMatch, kGroup = StageClock::kGroup, kFinish = StageClock::kFinish;
+    void clock_begin(Kind kind);
+    void clock_end(Kind kind);
     template <class F>
-    void timed(Kind kind, F&& launch);
+    void timed(Kind kind, F&& launch) {
+        clock_begin(kind);
+        launch();
+        clock_end(kind);
+    }
     void collect_timing();
     void count_match(int w, int h, const StageParams& sp);
+    struct Clock : StageClock {
+        Engine* e;
+        explicit Clock(Engine* en) : e(en) {}
+        void begin(Kind k) override { e->clock_begin(k); }
+        void end(Kind k) override { e->clock_end(k); }
+        void count_match(int w, int h, const StageParams& sp) override { e->count_match(w, h, sp); }
+    };
 
     Bm3dConfig cfg_;
     int device_ = 0;
@@ -112,9 +117,8 @@ private:
     DevPlane in_[3], refin_[3], basic_[3], out_[3];
     AccPlane acc_[3];
     StageScratch scratch_[3];
-    MatchBatch mbatch_;
-    GroupBatch gbatch_;
-    FinishBatch fbatch_;
+    std::unique_ptr<StageTables> tables_;
+    LaunchTunes tunes_;
     std::vector<void*> allocations_;
     struct PlanDeleter {
         void operator()(Plan* p) const;

@@ -288,16 +288,16 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
 }
 
 // Batched form: every job of every plane of the batch, a warp per group.
-template <int G, bool WIENER>
-__global__ void __launch_bounds__(32 * kWarps) group8_batch_kernel(const __grid_constant__ GroupBatch gb) {
+template <int G, bool WIENER, int NW>
+__global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_constant__ GroupBatch gb) {
     using Sh = Shape<G>;
     constexpr int CUBE = G * Sh::S;
-    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    __shared__ float smem[NW][WIENER ? 2 * CUBE : CUBE];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / Sh::LP;
-    const int stride_w = gridDim.x * kWarps;
+    const int stride_w = gridDim.x * NW;
     int pl = 0;
-    for (int job = blockIdx.x * kWarps + warp; job < gb.total_jobs; job += stride_w) {
+    for (int job = blockIdx.x * NW + warp; job < gb.total_jobs; job += stride_w) {
         while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= job) ++pl;
         const GroupPlane& P_ = gb.p[pl];
         const int lj = job - P_.job0;
@@ -327,11 +327,30 @@ void launch_gw(const GroupIO& io, const int32_t* pos, const int32_t* slot, const
     NSSB_CUDA(cudaGetLastError());
 }
 
-template <int G, bool W>
-void launch_batch_gw(const GroupBatch& gb, cudaStream_t stream) {
-    const int blocks = std::min(ceil_div(gb.total_jobs, kWarps), 148 * 16);
-    group8_batch_kernel<G, W><<<blocks, 32 * kWarps, 0, stream>>>(gb);
+template <int G, bool W, int NW>
+void launch_batch_gwn(const GroupBatch& gb, int ctas_per_sm, cudaStream_t stream) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        NSSB_CUDA(cudaGetDevice(&dev));
+        NSSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int blocks = std::min(ceil_div(gb.total_jobs, NW), sms * std::max(1, ctas_per_sm));
+    group8_batch_kernel<G, W, NW><<<blocks, 32 * NW, 0, stream>>>(gb);
     NSSB_CUDA(cudaGetLastError());
+}
+
+template <int G, bool W>
+void launch_batch_gw(const GroupBatch& gb, const GroupTune& t, cudaStream_t stream) {
+    switch (t.warps) {
+        case 2: launch_batch_gwn<G, W, 2>(gb, t.ctas_per_sm, stream); break;
+        case 8:
+            // 8 Wiener cubes of 16 patches exceed the 48 KB of static shared memory
+            if constexpr (G == 16 && W) launch_batch_gwn<G, W, 4>(gb, t.ctas_per_sm, stream);
+            else launch_batch_gwn<G, W, 8>(gb, t.ctas_per_sm, stream);
+            break;
+        default: launch_batch_gwn<G, W, 4>(gb, t.ctas_per_sm, stream); break;
+    }
 }
 
 }  // namespace
@@ -357,12 +376,15 @@ bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, c
     }
 }
 
-bool launch_group8_batch(const GroupBatch& gb, int group, bool wiener, cudaStream_t stream) {
+bool launch_group8_batch(const GroupBatch& gb, int group, bool wiener, cudaStream_t stream, const GroupTune* tune) {
     if (gb.total_jobs <= 0) return true;
+    const GroupTune t = tune ? *tune : GroupTune{};
     switch (group) {
-        case 4: wiener ? launch_batch_gw<4, true>(gb, stream) : launch_batch_gw<4, false>(gb, stream); return true;
-        case 8: wiener ? launch_batch_gw<8, true>(gb, stream) : launch_batch_gw<8, false>(gb, stream); return true;
-        case 16: wiener ? launch_batch_gw<16, true>(gb, stream) : launch_batch_gw<16, false>(gb, stream); return true;
+        case 4: wiener ? launch_batch_gw<4, true>(gb, t, stream) : launch_batch_gw<4, false>(gb, t, stream); return true;
+        case 8: wiener ? launch_batch_gw<8, true>(gb, t, stream) : launch_batch_gw<8, false>(gb, t, stream); return true;
+        case 16:
+            wiener ? launch_batch_gw<16, true>(gb, t, stream) : launch_batch_gw<16, false>(gb, t, stream);
+            return true;
         default: return false;
     }
 }

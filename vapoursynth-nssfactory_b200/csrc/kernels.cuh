@@ -28,11 +28,20 @@ struct MatchPlane {
 };
 struct MatchBatch {
     int n, step;
+    int total_ctas;    // tiles of the launch (set by the launcher)
+    int* queue;        // persistent form: next-tile counter, else null (set by the launcher)
     MatchPlane p[kMaxBatchPlanes];
+};
+// Launch shape of the 8x8 matcher; every choice gives the same lists.
+struct MatchTune {
+    int parts = 2;           // warp pairs splitting the window columns: 1, 2 or 4
+    int persistent = 0;      // 1: one resident wave taking tiles from a device counter
+    int* queue = nullptr;    // that counter (one int of device memory)
 };
 // The specialised exact matcher for 8x8 blocks (match8.cu) over a batch of
 // planes; false when the shape (bm_range, group, step) has no specialisation.
-bool launch_match8_batch(MatchBatch& batch, int bm_range, int group, cudaStream_t stream);
+bool launch_match8_batch(MatchBatch& batch, int bm_range, int group, cudaStream_t stream,
+                         const MatchTune* tune = nullptr);
 bool launch_match8(const float* plane, int64_t stride, int width, int height, int step, int bm_range, int group,
                    int32_t* pos, float* dist, int32_t* count, cudaStream_t stream);
 
@@ -54,9 +63,15 @@ struct GroupBatch {
     int n, total_jobs;
     GroupPlane p[kMaxBatchPlanes];
 };
+// Launch shape of the warp-per-group filter; every choice gives the same sums.
+struct GroupTune {
+    int warps = 4;          // groups (warps) per CTA: 2, 4 or 8
+    int ctas_per_sm = 16;   // grid = min(groups / warps, SMs x this); warps loop over the rest
+};
 // Warp-per-group filter for 8x8 blocks and groups of 4/8/16 over a batch of
 // planes (all Wiener or all hard threshold); false when the shape has none.
-bool launch_group8_batch(const GroupBatch& batch, int group, bool wiener, cudaStream_t stream);
+bool launch_group8_batch(const GroupBatch& batch, int group, bool wiener, cudaStream_t stream,
+                         const GroupTune* tune = nullptr);
 
 struct FinishPlane {
     long long* num;          // cleared by the kernel after use

@@ -60,26 +60,29 @@ constexpr int kPitch = 288;  // tile row pitch: >= 31 * 8 + 2 * 9 + 8 columns
 template <int R>
 __host__ __device__ constexpr int tile_rows() { return 2 * R + 8; }
 
+// Resident CTAs per SM the launch bounds ask for: 16 warps of 127 registers.
+template <int K, int P>
+__host__ __device__ constexpr int match8_min_blocks() { return (K <= 7 ? 16 : 12) / (2 * P) > 0 ? (K <= 7 ? 16 : 12) / (2 * P) : 1; }
+
+// One tile: 32 consecutive references of one grid row of one plane.
 template <int R, int K, int P>
-__global__ void __launch_bounds__(64 * P, (K <= 7 ? 4 : 3))
-    match8_kernel(const __grid_constant__ MatchBatch mb) {
+__device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, float* tile) {
     constexpr int B = 8, HB = 4;
     constexpr int NC = 2 * R + 1;            // candidates per window column
     constexpr int TR = tile_rows<R>();
     constexpr int CPW = (NC + P - 1) / P;    // window columns per warp pair
-    extern __shared__ float tile[];
     int pl = 0;
     {
         int lo = 0, hi = mb.n - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (mb.p[mid].cta0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+            if (mb.p[mid].cta0 <= tile_id) lo = mid; else hi = mid - 1;
         }
         pl = lo;
     }
     const MatchPlane& P_ = mb.p[pl];
     const int W = P_.W, H = P_.H, step = mb.step, nx = P_.nx;
-    const int local = blockIdx.x - P_.cta0;
+    const int local = tile_id - P_.cta0;
     const int chunks = (nx + kLanes - 1) / kLanes;
     const int ry = local / chunks, rx0 = (local - ry * chunks) * kLanes;
     const int rx1 = min(rx0 + kLanes, nx) - 1;
@@ -214,10 +217,27 @@ __global__ void __launch_bounds__(64 * P, (K <= 7 ? 4 : 3))
     P_.count[job] = 1 + n;
 }
 
-constexpr int kParts = 2;
+// Grid form: CTA b takes tile b. Persistent form (mb.queue set): a CTA takes
+// tile blockIdx.x, then keeps taking the next untaken tile from the device
+// counter until none is left; the counter is zero at launch.
+template <int R, int K, int P>
+__global__ void __launch_bounds__(64 * P, match8_min_blocks<K, P>())
+    match8_kernel(const __grid_constant__ MatchBatch mb) {
+    extern __shared__ float tile[];
+    __shared__ int next_tile;
+    int t = blockIdx.x;
+    while (t < mb.total_ctas) {
+        match8_tile<R, K, P>(mb, t, tile);
+        if (mb.queue == nullptr) break;
+        __syncthreads();  // the tile buffer is free again
+        if (threadIdx.x == 0) next_tile = atomicAdd(mb.queue, 1) + (int)gridDim.x;
+        __syncthreads();
+        t = next_tile;
+    }
+}
 
-template <int R, int K>
-void launch_rk(MatchBatch& mb, cudaStream_t stream) {
+template <int R, int K, int P>
+void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
     int ctas = 0;
     for (int i = 0; i < mb.n; ++i) {
         MatchPlane& p = mb.p[i];
@@ -226,35 +246,60 @@ void launch_rk(MatchBatch& mb, cudaStream_t stream) {
         p.cta0 = ctas;
         ctas += ceil_div(p.nx, kLanes) * p.ny;
     }
+    mb.total_ctas = ctas;
+    mb.queue = nullptr;
     if (ctas == 0) return;
     static_assert(31 * 8 + 2 * R + 8 <= kPitch, "tile pitch too small for this range");
-    const size_t smem = std::max((size_t)(kPitch * tile_rows<R>() + (2 * R + 1) * 64 * kParts) * sizeof(float),
-                                 (size_t)kParts * K * kLanes * sizeof(uint64_t));
-    auto kern = match8_kernel<R, K, kParts>;
+    const size_t smem = std::max((size_t)(kPitch * tile_rows<R>() + (2 * R + 1) * 64 * P) * sizeof(float),
+                                 (size_t)P * K * kLanes * sizeof(uint64_t));
+    auto kern = match8_kernel<R, K, P>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<ctas, 64 * kParts, smem, stream>>>(mb);
+    int grid = ctas;
+    if (tune.persistent && tune.queue) {
+        int dev = 0, sms = 0, per_sm = 0;
+        NSSB_CUDA(cudaGetDevice(&dev));
+        NSSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        NSSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 64 * P, smem));
+        const int resident = sms * std::max(per_sm, 1);
+        if (resident < ctas) {
+            grid = resident;
+            mb.queue = tune.queue;
+            NSSB_CUDA(cudaMemsetAsync(tune.queue, 0, sizeof(int), stream));
+        }
+    }
+    kern<<<grid, 64 * P, smem, stream>>>(mb);
     NSSB_CUDA(cudaGetLastError());
 }
 
+template <int R, int K>
+void launch_rk(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
+    switch (tune.parts) {
+        case 1: launch_rkp<R, K, 1>(mb, tune, stream); break;
+        case 4: launch_rkp<R, K, 4>(mb, tune, stream); break;
+        default: launch_rkp<R, K, 2>(mb, tune, stream); break;
+    }
+}
+
 template <int R>
-bool launch_r(MatchBatch& mb, int group, cudaStream_t stream) {
+bool launch_r(MatchBatch& mb, int group, const MatchTune& tune, cudaStream_t stream) {
     switch (group) {
-        case 2: launch_rk<R, 1>(mb, stream); return true;
-        case 4: launch_rk<R, 3>(mb, stream); return true;
-        case 8: launch_rk<R, 7>(mb, stream); return true;
-        case 16: launch_rk<R, 15>(mb, stream); return true;
+        case 2: launch_rk<R, 1>(mb, tune, stream); return true;
+        case 4: launch_rk<R, 3>(mb, tune, stream); return true;
+        case 8: launch_rk<R, 7>(mb, tune, stream); return true;
+        case 16: launch_rk<R, 15>(mb, tune, stream); return true;
         default: return false;
     }
 }
 
 }  // namespace
 
-bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t stream) {
+bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t stream, const MatchTune* tune) {
     if (mb.step < 1 || mb.step > 8 || mb.n < 1 || mb.n > kMaxBatchPlanes) return false;
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8) return false;
+    const MatchTune t = tune ? *tune : MatchTune{};
     switch (bm_range) {
-        case 9: return launch_r<9>(mb, group, stream);
+        case 9: return launch_r<9>(mb, group, t, stream);
         default: return false;
     }
 }
@@ -265,7 +310,7 @@ bool launch_match8(const float* plane, int64_t stride, int width, int height, in
     mb.n = 1;
     mb.step = step;
     mb.p[0] = MatchPlane{plane, stride, pos, dist, count, width, height, 0, 0, 0};
-    return launch_match8_batch(mb, bm_range, group, stream);
+    return launch_match8_batch(mb, bm_range, group, stream, nullptr);
 }
 
 }  // namespace nssb

@@ -43,6 +43,12 @@ __global__ void fill_ones_kernel(float* d, int64_t stride, int w, int h) {
 // One temporal stage (hard threshold, or Wiener with per-frame references).
 class TemporalStage {
 public:
+    // A new clip: nothing in the ring belongs to it.
+    void invalidate() {
+        for (int s = 0; s < kMaxSlots; ++s) target_[s] = -1;
+        next_c_ = 0;
+    }
+
     using Getter = std::function<void(int frame, const float* planes[3], int64_t strides[3])>;
 
     TemporalStage(const Bm3dConfig& cfg, const StageParams* sp, bool wiener, cudaStream_t stream)
@@ -297,6 +303,9 @@ public:
         best->index = idx;
         return best;
     }
+    void invalidate() {
+        for (auto& s : slots_) s.index = -1;
+    }
     void upload(DevFrameSet* s, const nssb_frame& f) {
         for (int p = 0; p < cfg_.planes; ++p)
             NSSB_CUDA(cudaMemcpy2DAsync(s->p[p], s->pitch[p] * 4, f.planes[p], f.strides[p] * 4,
@@ -315,6 +324,47 @@ struct Engine::Plan {
 };
 
 void Engine::PlanDeleter::operator()(Plan* p) const { delete p; }
+
+void Engine::reset_clip(int num_frames) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (num_frames < 1) throw std::invalid_argument("nss_cuda.BM3D: a clip needs at least one frame");
+    cfg_.vi.num_frames = num_frames;
+    cfg_.out_vi.num_frames = num_frames;
+    if (!plan_) return;
+    for (TemporalStage* st : {plan_->basic.get(), plan_->final.get()})
+        if (st) st->invalidate();
+    for (FrameCache* c : {plan_->src_cache.get(), plan_->ref_cache.get(), plan_->basic_cache.get()})
+        if (c) c->invalidate();
+}
+
+size_t Engine::footprint(const Bm3dConfig& cfg, bool host_frames) {
+    auto px = [&](int p) { return (size_t)((cfg.plane_w[p] + 31) / 32 * 32) * cfg.plane_h[p]; };
+    size_t total = 0, frame = 0;
+    const int r = cfg.radius;
+    for (int p = 0; p < cfg.planes; ++p) {
+        frame += px(p) * 4;
+        size_t jobs = 0, group = 0, cube = 0;
+        for (const StageParams* sp : {&cfg.final_stage[p], &cfg.basic_stage[p]}) {
+            jobs = std::max(jobs, (size_t)grid_count(cfg.plane_w[p], sp->block, sp->step) *
+                                      grid_count(cfg.plane_h[p], sp->block, sp->step));
+            group = std::max(group, (size_t)sp->group);
+            cube = std::max(cube, group_filter_scratch_floats(sp->block, sp->group, true));
+        }
+        // in, refin, basic, out + num, wsum + pos, slot, dist, count, cube
+        total += px(p) * (4 * 4 + 2 * 8) + jobs * group * 12 + jobs * 4 + cube * 4;
+        if (r > 0) {
+            // per temporal stage: 2r+1 target sums + match lists
+            const size_t stage = (2 * r + 1) * px(p) * 16 + jobs * group * 12 + jobs * 4 + cube * 4;
+            total += stage * (cfg.two_stage ? 2 : 1);
+        }
+    }
+    if (r > 0) {
+        size_t frames = cfg.two_stage ? 2 * r + 2 : 0;
+        if (host_frames) frames += 8 * r + 2 + (cfg.has_ref ? 4 * r + 2 : 0);
+        total += frames * frame;
+    }
+    return total;
+}
 
 void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
                             nssb_frame_out* out) {
