@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--served", type=int, default=2000, help="requests of the serving leg (0: skip it)")
+    ap.add_argument("--served-plain", type=int, default=300,
+                    help="requests of the same stream rendered by the per-frame drop-in for comparison")
     return ap.parse_args()
 
 
@@ -323,6 +326,10 @@ def our_arm(args):
                                "note": "plain form, one pass over the step's frames"},
         "clocks": clock,
     }
+    if args.served > 0:
+        out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain))
+        out["served"]["note"] = ("seeded Poisson arrivals at 200 req/s; latency = submission -> outputs in pinned "
+                                 "host memory; per rank")
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
@@ -339,6 +346,117 @@ def our_arm(args):
         print(json.dumps(out), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+SERVED_RES = {"480p": (854, 480), "720p": (1280, 720), "1080p": (1920, 1080), "2160p": (3840, 2160)}
+
+
+def served_workload(n_req, rate=200.0, seed=2024):
+    """Seeded Poisson arrivals (mean `rate` req/s) of 1-8 frame YUV420PS clips at
+    480p/720p/1080p/2160p, sigma 3/5/10/20, radius 0-2, final=1."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n_req)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    names = list(SERVED_RES)
+    return [dict(t=float(arrivals[i]), res=names[int(rng.integers(4))], frames=int(rng.integers(1, 9)),
+                 sigma=float(rng.choice([3.0, 5.0, 10.0, 20.0])), radius=int(rng.integers(0, 3)))
+            for i in range(n_req)]
+
+
+def served_leg(nssb, synth, local, n_req, n_plain):
+    """The serving form on the request stream above, then the per-frame drop-in
+    (a BM3D node per request, first come first served) on its first n_plain
+    requests with the same arrival times. Latency: arrival -> all outputs in
+    host memory."""
+    import queue
+    import threading
+
+    import torch
+
+    reqs = served_workload(n_req)
+    pool, outs, clips = {}, {}, {}
+    for i, (name, (w, h)) in enumerate(SERVED_RES.items()):
+        frames = synth.panning_clip(3000 + i, w, h, frames=8, sigma=10.0)
+        pool[name] = [tuple(torch.from_numpy(p).pin_memory().numpy() for p in f) for f in frames]
+        outs[name] = [tuple(torch.empty(p.shape, dtype=torch.float32).pin_memory().numpy() for p in f)
+                      for f in frames]
+        for k in range(1, 9):
+            clips[(name, k)] = nssb.Clip.from_frames(pool[name][:k], nssb.YUV, 1, 1)
+    srv = nssb.Server(device_id=local)
+    # warm-up: every (resolution, radius) once, so engines and kernels are loaded
+    for name in SERVED_RES:
+        for r in range(3):
+            srv.wait(srv.submit(clips[(name, 2)], outs=outs[name][:2], sigma=10.0, radius=r, final=1))
+    check_ids = [i for i, q in enumerate(reqs) if q["res"] == "480p"][:4]
+    check_out = {i: [tuple(np.empty_like(p) for p in f) for f in pool["480p"][:reqs[i]["frames"]]] for i in check_ids}
+    lat, qms, done_at = [], [], []
+    q = queue.Queue()
+
+    def waiter():
+        while True:
+            t = q.get()
+            if t is None:
+                return
+            _, res = srv.wait(t)
+            lat.append(res.latency_ms)
+            qms.append(res.queue_ms)
+            done_at.append(time.perf_counter())
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    for i, rq in enumerate(reqs):
+        wait = rq["t"] - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        o = check_out[i] if i in check_ids else outs[rq["res"]][:rq["frames"]]
+        q.put(srv.submit(clips[(rq["res"], rq["frames"])], outs=o, sigma=rq["sigma"], radius=rq["radius"], final=1))
+    q.put(None)
+    th.join()
+    span = max(done_at) - t0
+    st = srv.stats()
+    srv.close()
+    total_frames = sum(r["frames"] for r in reqs)
+    served = {"requests": n_req, "frames": total_frames, "fps": total_frames / span,
+              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+              "queue_p50_ms": float(np.percentile(qms, 50)), "queue_p99_ms": float(np.percentile(qms, 99)),
+              "span_s": span, "ticks": int(st.ticks), "tick_frames": int(st.tick_frames),
+              "temporal_frames": int(st.temporal_frames), "peak_active": int(st.peak_active),
+              "peak_reserved_gb": st.peak_reserved_bytes / 1e9, "budget_gb": st.budget_bytes / 1e9,
+              "engines_created": int(st.engines_created), "engines_reused": int(st.engines_reused)}
+    # the served outputs equal the drop-in's
+    same = True
+    for i in check_ids:
+        rq = reqs[i]
+        node = nssb.BM3D(clips[("480p", rq["frames"])], sigma=rq["sigma"], radius=rq["radius"], final=1,
+                         device_id=local)
+        for n in range(rq["frames"]):
+            same &= all(np.array_equal(a, b) for a, b in zip(node.get_frame(n), check_out[i][n]))
+        node.close()
+    served["served_equals_plain_bitwise"] = bool(same)
+    # the per-frame drop-in, first come first served, on the first n_plain requests
+    plat, pdone = [], []
+    t0 = time.perf_counter()
+    for rq in reqs[:n_plain]:
+        wait = rq["t"] - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        node = nssb.BM3D(clips[(rq["res"], rq["frames"])], sigma=rq["sigma"], radius=rq["radius"], final=1,
+                         device_id=local)
+        for n in range(rq["frames"]):
+            node.get_frame(n, out=outs[rq["res"]][n])
+        node.close()
+        now = time.perf_counter()
+        plat.append((now - t0 - rq["t"]) * 1e3)
+        pdone.append(now)
+    pframes = sum(r["frames"] for r in reqs[:n_plain])
+    served["plain"] = {"requests": n_plain, "frames": pframes, "fps": pframes / (max(pdone) - t0),
+                       "p50_ms": float(np.percentile(plat, 50)), "p99_ms": float(np.percentile(plat, 99))}
+    # the served form on the same first n_plain requests, for a like-for-like ratio
+    sub_lat = lat[:n_plain]
+    served["served_first_n"] = {"requests": n_plain, "p50_ms": float(np.percentile(sub_lat, 50)),
+                                "p99_ms": float(np.percentile(sub_lat, 99))}
+    return served
 
 
 def main():

@@ -216,6 +216,59 @@ int nssb_batch_run(nssb_batch* b, const nssb_batch_item* items, int n);
 int nssb_batch_get_info(nssb_batch* b, nssb_batch_info* out);
 void nssb_batch_free(nssb_batch* b);
 
+/* ---- serving form ----
+ * A request loop on one device. A request is a short clip with the
+ * arguments of nss_cuda.BM3D (any radius in rolling mode, final, chroma,
+ * sigma ...). Requests are admitted in arrival order while their device
+ * footprint fits the memory budget; admitted radius-0 requests are rendered
+ * together in continuously formed batches (requests arriving meanwhile join
+ * the next batch), radius > 0 requests on pooled engines whose window frames
+ * and rolling sums stay on the device, concurrently with the batches. Every
+ * output equals what nssb_bm3d_get_frame gives for the same clip and
+ * arguments, alone or in any mix. No reference counterpart: the reference
+ * serves frames through VapourSynth's frame threads
+ * (src/cuda/runtime/stream_pool.hpp:62-140). */
+typedef struct nssb_server nssb_server;
+typedef struct nssb_serve_request {
+    nssb_video_info vi;     /* the clip: format, size, num_frames = frames of the request */
+    const nssb_arg* args;   /* nss_cuda.BM3D arguments (device_id is the server's) */
+    int nargs;
+    const nssb_frame* clip; /* vi.num_frames frames */
+    const nssb_frame* ref;  /* vi.num_frames ref-clip frames (same format), or NULL */
+    int memory;             /* NSSB_MEM_HOST / NSSB_MEM_DEVICE for clip, ref and out */
+    nssb_frame_out* out;    /* vi.num_frames output frames; written when the request completes */
+} nssb_serve_request;
+typedef struct nssb_serve_result {
+    int status;              /* NSSB_OK or the request's error code */
+    int frames;
+    double queue_ms;         /* submission -> admission */
+    double latency_ms;       /* submission -> every output written */
+    int64_t footprint_bytes; /* device memory reserved at admission */
+    char error[192];         /* error text when status != NSSB_OK */
+} nssb_serve_result;
+typedef struct nssb_server_stats {
+    int64_t submitted, completed, failed, frames;
+    int64_t ticks, tick_frames, temporal_frames; /* batched ticks and their frames; radius > 0 frames */
+    int64_t queued, active, peak_active;
+    int64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
+    int64_t engines_created, engines_reused;
+} nssb_server_stats;
+/* args (ints): "memory_budget_mb" (default 0: 80 % of the free device memory),
+ * "max_tick_mpx" (pixels per batch, all planes, in millions; default 64),
+ * "workers" (radius > 0 requests in flight; default 4). */
+int nssb_server_create(int device_id, const nssb_arg* args, int nargs, nssb_server** out);
+/* Checks the arguments (creation errors carry nss_cuda.BM3D's messages) and
+ * queues the request. The request's frame arrays and planes must stay valid
+ * until its result has been collected by nssb_server_wait. */
+int nssb_server_submit(nssb_server* s, const nssb_serve_request* req, int64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit) and collects its result:
+ * NSSB_OK when it completed (its own status is in out->status),
+ * NSSB_ERR_TIMEOUT when the time ran out first (collect it later). */
+int nssb_server_wait(nssb_server* s, int64_t ticket, int64_t timeout_ms, nssb_serve_result* out);
+int nssb_server_get_stats(nssb_server* s, nssb_server_stats* out);
+/* Finishes the admitted work, fails what is still queued, releases everything. */
+void nssb_server_free(nssb_server* s);
+
 #ifdef __cplusplus
 }
 #endif

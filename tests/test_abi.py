@@ -62,3 +62,16 @@ def test_batch_create_checks_arguments_then_device(nssb):
     if not torch.cuda.is_available():
         with pytest.raises(nssb.Error, match="nss_batch: no CUDA device available"):
             nssb.Batch()
+
+
+def test_server_create_checks_arguments_then_device(nssb):
+    import pytest
+    import torch
+
+    with pytest.raises(nssb.Error, match="unknown argument bogus"):
+        nssb.Server(bogus=1)
+    with pytest.raises(nssb.Error, match="workers out of range"):
+        nssb.Server(workers=0)
+    if not torch.cuda.is_available():
+        with pytest.raises(nssb.Error, match="nss_server: no CUDA device available"):
+            nssb.Server()

@@ -108,6 +108,26 @@ class BatchInfo(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServeRequest(C.Structure):
+    _fields_ = [("vi", VideoInfo), ("args", C.POINTER(Arg)), ("nargs", C.c_int), ("clip", C.POINTER(Frame)),
+                ("ref", C.POINTER(Frame)), ("memory", C.c_int), ("out", C.POINTER(FrameOut))]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("frames", C.c_int), ("queue_ms", C.c_double), ("latency_ms", C.c_double),
+                ("footprint_bytes", C.c_int64), ("error", C.c_char * 192)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(f, C.c_int64) for f in (
+        "submitted", "completed", "failed", "frames", "ticks", "tick_frames", "temporal_frames", "queued", "active",
+        "peak_active", "budget_bytes", "reserved_bytes", "peak_reserved_bytes", "engines_created",
+        "engines_reused")]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 def lib():
     """The loaded library; raises if it is missing (no fallback)."""
     global _lib
@@ -143,6 +163,12 @@ def lib():
         L.nssb_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]
         L.nssb_batch_free.argtypes = [C.c_void_p]
         L.nssb_batch_free.restype = None
+        L.nssb_server_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
+        L.nssb_server_submit.argtypes = [C.c_void_p, C.POINTER(ServeRequest), C.POINTER(C.c_int64)]
+        L.nssb_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(ServeResult)]
+        L.nssb_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.nssb_server_free.argtypes = [C.c_void_p]
+        L.nssb_server_free.restype = None
         _lib = L
     return _lib
 
@@ -378,6 +404,68 @@ class Batch:
             results.append(out)
         check(lib().nssb_batch_run(self.handle, items, n))
         return results
+
+
+def _int_args(vals: dict):
+    arrs = [(C.c_int64 * 1)(int(v)) for v in vals.values()]
+    return (Arg * max(1, len(vals)))(*[Arg(k.encode(), ARG_INT, 1, a, None, None) for k, a in zip(vals, arrs)]), arrs
+
+
+class Server:
+    """The serving form: ``submit(clip, ref=None, **bm3d_args)`` queues a request
+    (a short clip, the arguments of BM3D) and returns a ticket; ``wait(ticket)``
+    returns (outputs, result). Requests are admitted by device footprint and
+    rendered in continuous batches (radius 0) or on pooled engines (radius > 0)."""
+
+    def __init__(self, device_id: int = 0, **opts):
+        args, self._keep = _int_args(opts)
+        h = C.c_void_p()
+        check(lib().nssb_server_create(device_id, args, len(opts), C.byref(h)))
+        self.handle = h
+        self._pending = {}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().nssb_server_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, clip: Clip, ref: Clip | None = None, outs=None, **kwargs) -> int:
+        n = clip.vi.num_frames
+        device = clip.device
+        frames = (Frame * n)(*[_frame_struct(f) for f in clip.frames])
+        refs = (Frame * n)(*[_frame_struct(f) for f in ref.frames]) if ref is not None else None
+        if outs is None:
+            shapes = [clip.vi.plane_shape(p) for p in range(clip.vi.planes())]
+            if device:
+                import torch
+
+                dev = clip.frames[0][0].device
+                outs = [tuple(torch.empty(sh, dtype=torch.float32, device=dev) for sh in shapes) for _ in range(n)]
+            else:
+                outs = [tuple(np.empty(sh, np.float32) for sh in shapes) for _ in range(n)]
+        fouts = (FrameOut * n)(*[_frame_struct(o, FrameOut) for o in outs])
+        args = _ArgBuffer(kwargs)
+        req = ServeRequest(clip.vi, args.array, args.count, frames, refs, MEM_DEVICE if device else MEM_HOST, fouts)
+        ticket = C.c_int64()
+        check(lib().nssb_server_submit(self.handle, C.byref(req), C.byref(ticket)))
+        self._pending[ticket.value] = (clip, ref, frames, refs, fouts, outs, args)
+        return ticket.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        res = ServeResult()
+        check(lib().nssb_server_wait(self.handle, ticket, timeout_ms, C.byref(res)))
+        outs = self._pending.pop(ticket)[5]
+        if res.status != OK:
+            raise Error(res.error.decode())
+        return outs, res
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().nssb_server_get_stats(self.handle, C.byref(st)))
+        return st
 
 
 def BM3D(clip: Clip, ref: Clip | None = None, **kwargs) -> Node:

@@ -4,6 +4,7 @@
 #include "nss_b200.h"
 
 #include "batch.hpp"
+#include "server.hpp"
 #include "engine.hpp"
 
 #include <cstdio>
@@ -18,6 +19,10 @@ struct nssb_bm3d {
 
 struct nssb_batch {
     std::unique_ptr<nssb::BatchEngine> engine;
+};
+
+struct nssb_server {
+    std::unique_ptr<nssb::Server> server;
 };
 
 namespace {
@@ -284,5 +289,58 @@ int nssb_batch_get_info(nssb_batch* b, nssb_batch_info* out) {
 }
 
 void nssb_batch_free(nssb_batch* b) { delete b; }
+
+int nssb_server_create(int device_id, const nssb_arg* args, int nargs, nssb_server** out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("nssb_server_create: out missing");
+        nssb::ServerOptions opt;
+        for (int i = 0; i < nargs; ++i) {
+            const nssb_arg& a = args[i];
+            const std::string key = a.key ? a.key : "";
+            if (key != "memory_budget_mb" && key != "max_tick_mpx" && key != "workers")
+                throw nssb::ArgumentError("nss_server: unknown argument " + key);
+            if (a.type != NSSB_ARG_INT || a.count != 1 || !a.ints)
+                throw nssb::ArgumentError("nss_server: " + key + " must be one int");
+            const int64_t v = a.ints[0];
+            if (v < 0 || (key != "memory_budget_mb" && v < 1) || (key == "workers" && v > 64))
+                throw nssb::ArgumentError("nss_server: " + key + " out of range");
+            if (key == "memory_budget_mb") opt.budget_bytes = (size_t)v << 20;
+            else if (key == "max_tick_mpx") opt.max_tick_mpx = (double)v;
+            else opt.workers = (int)v;
+        }
+        acquire_device(device_id, "nss_server");
+        auto h = std::make_unique<nssb_server>();
+        h->server = std::make_unique<nssb::Server>(device_id, opt);
+        *out = h.release();
+    });
+}
+
+int nssb_server_submit(nssb_server* s, const nssb_serve_request* req, int64_t* ticket) {
+    if (ticket) *ticket = 0;
+    return guarded([&] {
+        if (!s || !req || !ticket) throw std::invalid_argument("nssb_server_submit: invalid arguments");
+        *ticket = s->server->submit(*req);
+    });
+}
+
+int nssb_server_wait(nssb_server* s, int64_t ticket, int64_t timeout_ms, nssb_serve_result* out) {
+    int timed_out = 0;
+    const int rc = guarded([&] {
+        if (!s) throw std::invalid_argument("nssb_server_wait: invalid arguments");
+        timed_out = !s->server->wait(ticket, timeout_ms, out);
+    });
+    if (rc == NSSB_OK && timed_out) return fail(NSSB_ERR_TIMEOUT, "nssb_server_wait: timed out");
+    return rc;
+}
+
+int nssb_server_get_stats(nssb_server* s, nssb_server_stats* out) {
+    return guarded([&] {
+        if (!s || !out) throw std::invalid_argument("nssb_server_get_stats: invalid arguments");
+        s->server->stats(out);
+    });
+}
+
+void nssb_server_free(nssb_server* s) { delete s; }
 
 }  // extern "C"

@@ -148,9 +148,11 @@ std::string BatchPlan::signature_of(const BatchItem* items, int n) {
     return os.str();
 }
 
-void BatchPlan::layout(const BatchItem* items, int n) {
+void BatchPlan::layout(const BatchItem* items, int n, cudaStream_t stream) {
     std::string sig = signature_of(items, n);
     if (arena_ && sig == sig_) return;
+    NSSB_CUDA(cudaSetDevice(device_));
+    NSSB_CUDA(cudaStreamSynchronize(stream));  // the arena's previous layout is done with
     release_graph();
     sig_.clear();
     planes_.clear();
@@ -200,7 +202,6 @@ void BatchPlan::layout(const BatchItem* items, int n) {
             scratch_.push_back(sc);
         }
     }
-    NSSB_CUDA(cudaSetDevice(device_));
     if (off > arena_cap_) {
         if (arena_) dev_free(arena_);
         arena_ = nullptr;
@@ -211,7 +212,7 @@ void BatchPlan::layout(const BatchItem* items, int n) {
     if (!queue_) queue_ = static_cast<int*>(dev_alloc(256));
     arena_bytes_ = off;
     // num must start at zero; every finish leaves it zero again
-    NSSB_CUDA(cudaMemset(arena_, 0, off));
+    NSSB_CUDA(cudaMemsetAsync(arena_, 0, off, stream));
     auto F = [&](size_t o) { return o == kNone ? nullptr : reinterpret_cast<float*>(arena_ + o); };
     for (size_t k = 0; k < planes_.size(); ++k) {
         const Plane& pl = planes_[k];
@@ -441,8 +442,8 @@ void BatchEngine::run(const BatchItem* items, int n) {
             cudaStream_t s = streams_[lane];
             const BatchItem* c = items + parts[k].first;
             const int m = parts[k].second;
-            BatchPlan& plan = plan_for(BatchPlan::signature_of(c, m), lane);
-            plan.layout(c, m);
+            BatchPlan& plan = plan_for(opt_.plan_per_stream ? std::string() : BatchPlan::signature_of(c, m), lane);
+            plan.layout(c, m, s);
             LaunchTunes t = opt_.fixed;
             const bool need_tune = opt_.autotune && tuned_.find(plan.signature()) == tuned_.end();
             if (opt_.autotune && !need_tune) t = tuned_[plan.signature()];

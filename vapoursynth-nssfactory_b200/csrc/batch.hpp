@@ -62,8 +62,9 @@ public:
     BatchPlan(const BatchPlan&) = delete;
     BatchPlan& operator=(const BatchPlan&) = delete;
 
-    // Lays the batch out; keeps the arena (and graph) when the layout is unchanged.
-    void layout(const BatchItem* items, int n);
+    // Lays the batch out; keeps the arena (and graph) when the layout is
+    // unchanged. A new layout first waits for the plan's work on `s`.
+    void layout(const BatchItem* items, int n, cudaStream_t s);
     static std::string signature_of(const BatchItem* items, int n);
     const std::string& signature() const { return sig_; }
     size_t arena_bytes() const { return arena_bytes_; }
@@ -101,6 +102,7 @@ struct BatchOptions {
     bool autotune = true;
     bool graphs = true;
     int chunk_frames = 0;  // 0: one chunk for device items, up to 4 equal chunks with host items
+    bool plan_per_stream = false;  // one plan per stream, re-laid out as layouts change (serving)
     LaunchTunes fixed;     // the launch shapes used when autotune is off
 };
 
