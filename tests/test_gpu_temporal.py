@@ -40,6 +40,9 @@ def gray_clip(synth, n, w, h, sigma, seed=4):
 @pytest.mark.parametrize("block,group,rng_,radius,ps_num,ps_range,valid", [
     (8, 8, 9, 2, 2, 4, (0, -1)), (8, 16, 5, 1, 3, 3, (1, -1)), (4, 8, 6, 2, 2, 2, (0, 4)),
     (8, 4, 7, 2, 1, 4, (2, 5)), (16, 8, 5, 1, 2, 2, (0, -1)), (12, 32, 4, 1, 4, 3, (0, -1)),
+    # the 8x8 fast path at its limits: 8 seeds, wide windows clamped at the edges, radius 3, groups 2 and 16
+    (8, 8, 9, 3, 5, 7, (0, -1)), (8, 16, 9, 2, 8, 2, (1, 4)), (8, 2, 9, 1, 1, 12, (0, -1)),
+    (8, 16, 6, 2, 4, 12, (0, -1)),
 ])
 def test_match_temporal_exact(nssb, oracle, synth, dev, block, group, rng_, radius, ps_num, ps_range, valid):
     ntemp = 2 * radius + 1
