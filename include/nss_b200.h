@@ -137,6 +137,27 @@ int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stat
 int nssb_match_spatial(const float* plane, int64_t stride, int width, int height, int block, int step,
                        int bm_range, int group, int32_t* pos, float* dist, int32_t* count, void* stream);
 
+/* Precision form of nssb_match_spatial for 8x8 blocks and bm_range 9 (groups
+ * 2, 4, 8, 16): candidate distances |r|^2 + |c|^2 - 2 r.c with the dot
+ * products on the tensor cores (tcgen05.mma, BF16 hi/lo split of every pixel,
+ * FP32 accumulation in tensor memory), then every candidate within a proven
+ * error margin of the K-th distance re-ranked with the exact FP32 distance,
+ * so pos, dist and count equal nssb_match_spatial's bit for bit. stats (may
+ * be NULL) receives the re-rank accounting of this call. Returns
+ * NSSB_ERR_STATE for shapes it does not cover, NSSB_ERR_TIMEOUT if a bounded
+ * device wait gave up. No reference counterpart in this form: the
+ * reference's tensor matcher (src/cuda/common/match.cu, mma.sync, large
+ * windows) orders ties differently (src/cuda/common/match.hpp:2-8). */
+typedef struct nssb_tc_stats {
+    int64_t survivors;      /* candidates re-ranked exactly */
+    int64_t refs;           /* references matched */
+    float max_error_ratio;  /* largest |approximate - exact| / margin among survivors (must stay < 1) */
+    int flagged_tiles;      /* tiles with non-finite pixels (every candidate re-ranked) */
+    int timeouts;           /* bounded device waits that gave up */
+} nssb_tc_stats;
+int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int group,
+                          int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats, void* stream);
+
 /* Predictive temporal matching (collect_temporal, matcher.hpp:319-373; device
  * form match.cu:1707-1757). planes/strides: host arrays of ntemp device
  * planes; reference slot t0; valid slots [valid_begin, valid_end). slot[j*group+q]
@@ -255,7 +276,7 @@ typedef struct nssb_server_stats {
 } nssb_server_stats;
 /* args (ints): "memory_budget_mb" (default 0: 80 % of the free device memory),
  * "max_tick_mpx" (pixels per batch, all planes, in millions; default 64),
- * "workers" (radius > 0 requests in flight; default 4). */
+ * "workers" (radius > 0 requests in flight; default 8). */
 int nssb_server_create(int device_id, const nssb_arg* args, int nargs, nssb_server** out);
 /* Checks the arguments (creation errors carry nss_cuda.BM3D's messages) and
  * queues the request. The request's frame arrays and planes must stay valid

@@ -1,0 +1,115 @@
+"""Precision form of the 8x8 matcher (tensor-core distances + exact re-rank):
+its lists must equal the FP32 matcher's bit for bit -- positions, distances
+and counts -- on textured, noisy, flat (all ties) and non-finite images, at
+every step and group size it covers, and its re-rank margin must hold
+(largest |approximate - exact| / margin below 1)."""
+import ctypes as C
+import importlib
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def synth():
+    return importlib.import_module("vapoursynth-nssfactory_b200.synth")
+
+
+def grid(n, b, s):
+    return (n - b + s - 1) // s + 1
+
+
+def run_both(nssb, img, dev, step=8, group=8):
+    h, w = img.shape
+    plane = torch.from_numpy(np.ascontiguousarray(img, np.float32)).to(dev)
+    jobs = grid(w, 8, step) * grid(h, 8, step)
+    out = []
+    stats = nssb.TcStats()
+    for tc in (False, True):
+        pos = torch.full((jobs, group), -7, dtype=torch.int32, device=dev)
+        dist = torch.full((jobs, group), -7.0, dtype=torch.float32, device=dev)
+        cnt = torch.zeros(jobs, dtype=torch.int32, device=dev)
+        if tc:
+            rc = nssb.lib().nssb_match_spatial_tc(plane.data_ptr(), w, w, h, step, group, pos.data_ptr(),
+                                                  dist.data_ptr(), cnt.data_ptr(), C.byref(stats), None)
+        else:
+            rc = nssb.lib().nssb_match_spatial(plane.data_ptr(), w, w, h, 8, step, 9, group, pos.data_ptr(),
+                                               dist.data_ptr(), cnt.data_ptr(), None)
+        nssb.check(rc)
+        torch.cuda.synchronize()
+        out.append((pos.cpu().numpy(), dist.cpu().numpy(), cnt.cpu().numpy()))
+    return out, stats
+
+
+def assert_equal_lists(out):
+    (p0, d0, c0), (p1, d1, c1) = out
+    assert np.array_equal(c0, c1)
+    assert np.array_equal(p0, p1)
+    assert np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+
+
+def test_small_plane_first(nssb, synth, dev):
+    img = synth.gray_frame(3, 64, 48, 10)[0]
+    out, st = run_both(nssb, img, dev)
+    assert st.timeouts == 0
+    assert_equal_lists(out)
+    assert st.refs == 8 * 6 and 0 <= st.max_error_ratio < 1.0
+
+
+@pytest.mark.parametrize("w,h,step,group,sigma", [
+    (160, 96, 8, 8, 10), (200, 120, 4, 8, 5), (131, 77, 8, 16, 20), (96, 64, 3, 4, 10), (256, 40, 8, 2, 3),
+    (150, 90, 1, 8, 10), (513, 61, 7, 16, 5),
+])
+def test_equals_fp32_matcher(nssb, synth, dev, w, h, step, group, sigma):
+    img = synth.gray_frame(w * 7 + h, w, h, sigma)[0]
+    out, st = run_both(nssb, img, dev, step, group)
+    assert st.timeouts == 0 and st.flagged_tiles == 0
+    assert_equal_lists(out)
+    assert st.max_error_ratio < 1.0
+    assert st.survivors < 40 * st.refs  # the re-rank stays a small share of the window
+
+
+def test_flat_image_all_ties(nssb, dev):
+    img = np.full((72, 88), 0.25, np.float32)
+    out, st = run_both(nssb, img, dev)
+    assert_equal_lists(out)
+
+
+def test_quantised_image_many_ties(nssb, dev):
+    rng = np.random.default_rng(5)
+    img = (rng.integers(0, 4, (80, 120)) / 4.0).astype(np.float32)
+    out, st = run_both(nssb, img, dev, group=16)
+    assert_equal_lists(out)
+
+
+def test_non_finite_pixels_take_the_exact_path(nssb, synth, dev):
+    img = synth.gray_frame(11, 96, 64, 10)[0]
+    img[10, 20] = np.nan
+    img[40, 70] = np.inf
+    out, st = run_both(nssb, img, dev)
+    assert st.flagged_tiles > 0
+    assert_equal_lists(out)
+
+
+def test_large_values(nssb, synth, dev):
+    img = synth.gray_frame(12, 120, 80, 10)[0] * 1000.0 + 500.0
+    out, st = run_both(nssb, img, dev)
+    assert_equal_lists(out)
+    assert st.max_error_ratio < 1.0
+
+
+def test_1080p_plane(nssb, synth, dev):
+    img = synth.yuv420_clip(9, 1920, 1080, 1, 5.0)[0][0]
+    out, st = run_both(nssb, img, dev)
+    assert_equal_lists(out)
+    assert st.max_error_ratio < 1.0

@@ -93,6 +93,14 @@ class KernelStats(C.Structure):
 _lib = None
 
 
+class TcStats(C.Structure):
+    _fields_ = [("survivors", C.c_int64), ("refs", C.c_int64), ("max_error_ratio", C.c_float),
+                ("flagged_tiles", C.c_int), ("timeouts", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class BatchItem(C.Structure):
     _fields_ = [("node", C.c_void_p), ("clip", C.POINTER(Frame)), ("ref", C.POINTER(Frame)), ("memory", C.c_int),
                 ("out", C.POINTER(FrameOut))]
@@ -158,6 +166,8 @@ def lib():
                                             C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.nssb_bm3d_plane_stage_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                                     C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
         L.nssb_batch_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
         L.nssb_batch_run.argtypes = [C.c_void_p, C.POINTER(BatchItem), C.c_int]
         L.nssb_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]

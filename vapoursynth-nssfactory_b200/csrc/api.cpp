@@ -175,6 +175,40 @@ int nssb_match_spatial(const float* plane, int64_t stride, int width, int height
     });
 }
 
+int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int group,
+                          int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats, void* stream) {
+    int timeouts = 0;
+    const int rc = guarded([&] {
+        if (!plane || !pos || !count || width < 8 || height < 8 || step < 1 || step > 8 || stride < width)
+            throw std::invalid_argument("nss_cuda: invalid matching arguments");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        nssb::TcCounters* ctr = nullptr;
+        NSSB_CUDA(cudaMallocAsync(&ctr, sizeof(nssb::TcCounters), s));
+        NSSB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(nssb::TcCounters), s));
+        auto mb = std::make_unique<nssb::MatchBatch>();
+        mb->n = 1;
+        mb->step = step;
+        mb->p[0] = nssb::MatchPlane{plane, stride, pos, dist, count, width, height, 0, 0, 0};
+        const bool ok = nssb::launch_match_tc_batch(*mb, 9, group, ctr, s);
+        nssb::TcCounters host{};
+        if (ok) NSSB_CUDA(cudaMemcpyAsync(&host, ctr, sizeof host, cudaMemcpyDeviceToHost, s));
+        NSSB_CUDA(cudaFreeAsync(ctr, s));
+        NSSB_CUDA(cudaStreamSynchronize(s));
+        if (!ok) throw std::invalid_argument("nss_cuda: the precision matcher covers 8x8 blocks, bm_range 9, groups 2/4/8/16");
+        timeouts = (int)host.timeouts;
+        if (stats) {
+            stats->survivors = (int64_t)host.survivors;
+            stats->refs = (int64_t)host.refs;
+            uint32_t bits = host.max_ratio_bits;
+            std::memcpy(&stats->max_error_ratio, &bits, 4);
+            stats->flagged_tiles = (int)host.flagged_tiles;
+            stats->timeouts = (int)host.timeouts;
+        }
+    });
+    if (rc == NSSB_OK && timeouts > 0) return fail(NSSB_ERR_TIMEOUT, "nss_cuda: a device wait of the precision matcher gave up");
+    return rc;
+}
+
 int nssb_match_temporal(const float* const* planes, const int64_t* strides, int ntemp, int t0, int valid_begin,
                         int valid_end, int width, int height, int block, int step, int bm_range, int group,
                         int ps_num, int ps_range, int32_t* pos, int32_t* slot, float* dist, int32_t* count,

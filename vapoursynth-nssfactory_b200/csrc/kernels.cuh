@@ -45,6 +45,17 @@ bool launch_match8_batch(MatchBatch& batch, int bm_range, int group, cudaStream_
 bool launch_match8(const float* plane, int64_t stride, int width, int height, int step, int bm_range, int group,
                    int32_t* pos, float* dist, int32_t* count, cudaStream_t stream);
 
+// Precision form of the 8x8 matcher (match_tc.cu): BF16 tensor-core distances,
+// exact FP32 re-rank; the same lists as launch_match8_batch. Counters (device
+// memory, accumulated across launches): survivors re-ranked, references,
+// tiles with non-finite pixels, the largest |approx - exact| / margin seen,
+// and barrier waits that gave up (0 unless the device misbehaves).
+struct TcCounters {
+    unsigned long long survivors, refs;
+    unsigned int max_ratio_bits, flagged_tiles, timeouts, pad;
+};
+bool launch_match_tc_batch(MatchBatch& batch, int bm_range, int group, TcCounters* counters, cudaStream_t stream);
+
 struct GroupPlane {
     const float* src;
     const float* ref;  // Wiener reference, or null

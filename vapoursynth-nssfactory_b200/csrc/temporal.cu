@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(64 * kTRefs, 2)
     uint64_t best[64];
     int nb = 0;
     auto push = [&](uint64_t v) {
-        if (nb == G - 1 && !(v < best[nb - 1])) return;
+        if (nb > 0 && nb == G - 1 && !(v < best[nb - 1])) return;
         int p = nb < G - 1 ? nb++ : nb - 1;
         while (p > 0 && v < best[p - 1]) {
             best[p] = best[p - 1];
