@@ -345,6 +345,8 @@ BatchEngine::BatchEngine(int device, const BatchOptions& opt) : device_(device),
 }
 
 BatchEngine::~BatchEngine() {
+    for (auto& st : streams_)
+        if (st) (void)cudaStreamSynchronize(st);
     plans_.clear();
     (void)cudaEventDestroy(t0_);
     for (auto& e : t1_) (void)cudaEventDestroy(e);

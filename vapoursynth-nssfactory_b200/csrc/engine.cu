@@ -3,14 +3,54 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cstring>
 
 namespace nssb {
 
+namespace {
+
+// The library's device memory: one stream-ordered pool per device that keeps
+// what is freed (release threshold: unlimited), served on a private stream.
+// Creating and destroying engines then neither blocks on cudaMalloc's device
+// synchronisation nor stalls other streams the way cudaFree does.
+struct DevicePool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+DevicePool& device_pool(int dev) {
+    static std::mutex mu;
+    static std::map<int, DevicePool> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    DevicePool& d = pools[dev];
+    if (!d.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        NSSB_CUDA(cudaMemPoolCreate(&d.pool, &props));
+        uint64_t keep = ~0ull;
+        NSSB_CUDA(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        NSSB_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    }
+    return d;
+}
+
+}  // namespace
+
+// Memory from dev_alloc is ready for any stream when it returns. dev_free
+// requires that no queued work still uses the block (callers synchronise
+// their streams first).
 void* dev_alloc(size_t bytes) {
     void* p = nullptr;
     if (bytes == 0) return nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
+    int dev = 0;
+    NSSB_CUDA(cudaGetDevice(&dev));
+    DevicePool& d = device_pool(dev);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, d.pool, d.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d.stream);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         throw std::bad_alloc();
@@ -19,7 +59,12 @@ void* dev_alloc(size_t bytes) {
 }
 
 void dev_free(void* p) {
-    if (p) (void)cudaFree(p);
+    if (!p) return;
+    cudaPointerAttributes attr{};
+    int dev = 0;
+    if (cudaPointerGetAttributes(&attr, p) == cudaSuccess) dev = attr.device;
+    (void)cudaGetLastError();
+    (void)cudaFreeAsync(p, device_pool(dev).stream);
 }
 
 namespace {
@@ -41,6 +86,7 @@ Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg), tables_(new StageTables) {
 }
 
 void Engine::release() {
+    if (stream_) (void)cudaStreamSynchronize(stream_);  // nothing queued may still use the buffers
     for (auto& e : event_pool_) {
         (void)cudaEventDestroy(e.first);
         (void)cudaEventDestroy(e.second);
@@ -73,7 +119,7 @@ void Engine::alloc() {
         acc_[p].pitch = pitch;
         acc_[p].num = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
         acc_[p].wsum = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
-        NSSB_CUDA(cudaMemset(acc_[p].num, 0, (size_t)pitch * h * sizeof(long long)));
+        NSSB_CUDA(cudaMemsetAsync(acc_[p].num, 0, (size_t)pitch * h * sizeof(long long), stream_));
         size_t jobs = 0, group = 0, cube = 0;
         for (const StageParams* sp : {&cfg_.final_stage[p], &cfg_.basic_stage[p]}) {
             jobs = std::max(jobs, (size_t)grid_count(w, sp->block, sp->step) * grid_count(h, sp->block, sp->step));

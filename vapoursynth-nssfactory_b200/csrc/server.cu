@@ -28,6 +28,15 @@ std::string engine_key(const Bm3dConfig& c, int memory) {
     return os.str();
 }
 
+int64_t plane_pitch(int w) { return (int64_t)((w + 31) / 32 * 32); }
+
+// Device copies of a host request's frames: clip (+ ref) and outputs.
+size_t staging_bytes(const Bm3dConfig& c, int frames, bool ref) {
+    size_t frame = 0;
+    for (int p = 0; p < c.planes; ++p) frame += (size_t)plane_pitch(c.plane_w[p]) * c.plane_h[p] * 4;
+    return frame * frames * (ref ? 3 : 2);
+}
+
 double frame_mpx(const Bm3dConfig& c) {
     double px = 0;
     for (int p = 0; p < c.planes; ++p) px += (double)c.plane_w[p] * c.plane_h[p];
@@ -94,12 +103,14 @@ int64_t Server::submit(const nssb_serve_request& req) {
     r->clip.assign(req.clip, req.clip + r->frames);
     if (req.ref) r->ref.assign(req.ref, req.ref + r->frames);
     r->out.assign(req.out, req.out + r->frames);
-    r->key = engine_key(r->cfg, r->memory);
+    r->key = engine_key(r->cfg, NSSB_MEM_DEVICE);  // temporal engines always work on device frames
     if (r->cfg.radius == 0) {
         std::vector<BatchItem> items((size_t)r->frames, BatchItem{&r->cfg, nullptr, nullptr, r->memory, nullptr});
         r->footprint = BatchPlan::footprint(items.data(), r->frames);
     } else {
-        r->footprint = Engine::footprint(r->cfg, r->memory == NSSB_MEM_HOST);
+        // a pooled engine working on device frames + the request's frames staged on the device
+        r->footprint = Engine::footprint(r->cfg, false);
+        if (r->memory == NSSB_MEM_HOST) r->footprint += staging_bytes(r->cfg, r->frames, !r->ref.empty());
     }
     r->submitted = Clock::now();
     {
@@ -234,6 +245,12 @@ void Server::return_engine(const std::string& key, std::unique_ptr<Engine> e, si
 // One radius > 0 request at a time per worker, on a pooled engine.
 void Server::worker() {
     (void)cudaSetDevice(device_);
+    cudaStream_t stream = nullptr;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return;
+    struct Release {
+        cudaStream_t s;
+        ~Release() { (void)cudaStreamDestroy(s); }
+    } release{stream};
     for (;;) {
         Ptr r;
         {
@@ -249,15 +266,49 @@ void Server::worker() {
         int status = NSSB_OK;
         std::string error;
         std::unique_ptr<Engine> e;
+        void* stage = nullptr;
         try {
             e = take_engine(*r);
             e->reset_clip(r->frames);
+            const Bm3dConfig& c = r->cfg;
+            const bool host = r->memory == NSSB_MEM_HOST;
+            std::vector<nssb_frame> dclip(r->clip), dref(r->ref);
+            std::vector<nssb_frame_out> dout(r->out);
+            if (host) {
+                // the whole clip goes to the device once; outputs come back as they finish
+                stage = dev_alloc(staging_bytes(c, r->frames, !r->ref.empty()));
+                char* at = static_cast<char*>(stage);
+                auto place = [&](auto& frame, const auto* src, cudaMemcpyKind kind) {
+                    for (int p = 0; p < c.planes; ++p) {
+                        const int64_t pitch = plane_pitch(c.plane_w[p]);
+                        float* dst = reinterpret_cast<float*>(at);
+                        at += (size_t)pitch * c.plane_h[p] * 4;
+                        if (src)
+                            NSSB_CUDA(cudaMemcpy2DAsync(dst, pitch * 4, src->planes[p], src->strides[p] * 4,
+                                                        c.plane_w[p] * 4, c.plane_h[p], kind, stream));
+                        frame.planes[p] = dst;
+                        frame.strides[p] = pitch;
+                    }
+                };
+                for (int f = 0; f < r->frames; ++f) {
+                    place(dclip[f], &r->clip[f], cudaMemcpyHostToDevice);
+                    if (!r->ref.empty()) place(dref[f], &r->ref[f], cudaMemcpyHostToDevice);
+                    place(dout[f], static_cast<const nssb_frame*>(nullptr), cudaMemcpyHostToDevice);
+                }
+                NSSB_CUDA(cudaStreamSynchronize(stream));
+            }
             for (int f = 0; f < r->frames; ++f) {
-                e->get_frame(f, r->clip.data(), r->ref.empty() ? nullptr : r->ref.data(), 0, r->frames, r->memory,
-                             &r->out[f]);
+                e->get_frame(f, dclip.data(), dref.empty() ? nullptr : dref.data(), 0, r->frames, NSSB_MEM_DEVICE,
+                             &dout[f]);
+                if (host)
+                    for (int p = 0; p < c.planes; ++p)
+                        NSSB_CUDA(cudaMemcpy2DAsync(r->out[f].planes[p], r->out[f].strides[p] * 4, dout[f].planes[p],
+                                                    dout[f].strides[p] * 4, c.plane_w[p] * 4, c.plane_h[p],
+                                                    cudaMemcpyDeviceToHost, stream));
                 std::lock_guard<std::mutex> lock(mu_);
                 ++st_.temporal_frames;
             }
+            NSSB_CUDA(cudaStreamSynchronize(stream));
         } catch (const CudaError& ex) {
             status = NSSB_ERR_CUDA;
             error = ex.what();
@@ -268,7 +319,9 @@ void Server::worker() {
             status = NSSB_ERR_STATE;
             error = ex.what();
         }
-        if (e && status == NSSB_OK) return_engine(r->key, std::move(e), r->footprint);
+        (void)cudaStreamSynchronize(stream);
+        if (stage) dev_free(stage);
+        if (e && status == NSSB_OK) return_engine(r->key, std::move(e), Engine::footprint(r->cfg, false));
         e.reset();
         std::lock_guard<std::mutex> lock(mu_);
         complete_locked(r, status, error);

@@ -32,7 +32,7 @@ namespace nssb {
 struct ServerOptions {
     size_t budget_bytes = 0;   // 0: 80 % of the device memory free at creation
     double max_tick_mpx = 64;  // pixels (all planes) a tick renders at most
-    int workers = 4;           // radius > 0 requests in flight
+    int workers = 8;           // radius > 0 requests in flight
 };
 
 class Server {

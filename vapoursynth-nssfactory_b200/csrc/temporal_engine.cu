@@ -461,6 +461,7 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
         }
         NSSB_CUDA(cudaStreamSynchronize(stream_));
     } catch (...) {
+        (void)cudaStreamSynchronize(stream_);
         for (void* p : tmp) dev_free(p);
         throw;
     }
@@ -468,6 +469,7 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
 }
 
 Engine::~Engine() {
+    if (stream_) (void)cudaStreamSynchronize(stream_);
     plan_.reset();
     release();
 }
