@@ -123,8 +123,18 @@ typedef struct nssb_kernel_stats {
     double match_ms, group_ms, finish_ms; /* summed event durations (timing on) */
     double match_flops;      /* algorithmic matcher flops of the counted launches */
     double match_pairs;      /* reference-candidate pairs evaluated */
+    int64_t tc_survivors;    /* precision form: candidates re-ranked exactly */
+    int64_t tc_refs;         /* precision form: references matched */
+    double tc_max_error_ratio; /* precision form: largest |approximate - exact| / margin */
 } nssb_kernel_stats;
 int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stats* out);
+
+/* Matcher of a handle's 8x8 stages (spatial and the centre frame of
+ * temporal): 0 = FP32 (default), 1 = the tensor-core precision form of
+ * nssb_match_spatial_tc. Outputs are bit-identical either way. */
+#define NSSB_MATCHER_FP32 0
+#define NSSB_MATCHER_TENSOR 1
+int nssb_bm3d_set_matcher(nssb_bm3d* h, int form);
 
 /* ---- stage primitives on device memory (the kernels the filter runs) ----
  * Strides are in elements. stream is a cudaStream_t (NULL = default). */
@@ -213,6 +223,7 @@ typedef struct nssb_batch_item {
 } nssb_batch_item;
 typedef struct nssb_batch_info {
     int match_parts, match_persistent;  /* matcher shape in use */
+    int match_form;                     /* 0: FP32 matcher, 1: tensor-core precision form (same lists) */
     int group_warps, group_ctas_per_sm; /* group-filter shape in use */
     int graphs;                         /* 1: runs replay a captured graph */
     int64_t runs, frames;               /* batches and frames rendered */
@@ -226,7 +237,8 @@ typedef struct nssb_batch_info {
  * (frames per chunk; default 0: one chunk when every item is on the device,
  * else up to four equal chunks on two streams so that host copies overlap
  * the kernels), and the shapes
- * used when autotune is 0: "match_parts" (1, 2, 4; default 2),
+ * used when autotune is 0: "match_form" (0 FP32, 1 tensor-core precision
+ * form; default 0), "match_parts" (1, 2, 4; default 2),
  * "match_persistent" (0/1; default 0), "group_warps" (2, 4, 8; default 4),
  * "group_ctas_per_sm" (1..64; default 16). */
 int nssb_batch_create(int device_id, const nssb_arg* args, int nargs, nssb_batch** out);

@@ -115,6 +115,7 @@ def test_chunked_two_stream_runs(nssb, nodes, chunk):
     dict(match_parts=2, match_persistent=1, group_warps=4, group_ctas_per_sm=8),
     dict(match_parts=4, match_persistent=1, group_warps=8, group_ctas_per_sm=16),
     dict(match_parts=4, match_persistent=0, group_warps=8, group_ctas_per_sm=1),
+    dict(match_form=1, match_parts=2, match_persistent=0, group_warps=4, group_ctas_per_sm=16),
 ])
 @pytest.mark.parametrize("graph", [False, True])
 def test_launch_shapes_identical(nssb, synth, nodes, shape, graph):
@@ -128,6 +129,7 @@ def test_launch_shapes_identical(nssb, synth, nodes, shape, graph):
     info = b.info()
     assert (info.match_parts, info.match_persistent, info.group_warps, info.group_ctas_per_sm) == (
         shape["match_parts"], shape["match_persistent"], shape["group_warps"], shape["group_ctas_per_sm"])
+    assert info.match_form == shape.get("match_form", 0)
     b.close()
     big.close()
 

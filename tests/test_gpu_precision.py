@@ -113,3 +113,19 @@ def test_1080p_plane(nssb, synth, dev):
     out, st = run_both(nssb, img, dev)
     assert_equal_lists(out)
     assert st.max_error_ratio < 1.0
+
+
+def test_engine_precision_form_same_frames(nssb, synth, dev):
+    # spatial two-stage YUV420 and temporal (radius 1 and 2): the precision form gives the same bits
+    frames = synth.panning_clip(21, 160, 96, frames=5, sigma=10)
+    clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
+    for kw in (dict(sigma=10, final=1), dict(sigma=10, radius=1, final=1), dict(sigma=[10, 6, 6], radius=2)):
+        a, b = nssb.BM3D(clip, **kw), nssb.BM3D(clip, **kw)
+        b.set_matcher(1)
+        for n in range(5):
+            for pa, pb in zip(a.get_frame(n), b.get_frame(n)):
+                assert np.array_equal(pa, pb)
+        st = b.stats(False, False)
+        assert st.tc_refs > 0 and st.tc_max_error_ratio < 1.0
+        a.close()
+        b.close()

@@ -84,7 +84,8 @@ class FrameOut(C.Structure):
 class KernelStats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("match_launches", C.c_int64), ("group_launches", C.c_int64),
                 ("finish_launches", C.c_int64), ("match_ms", C.c_double), ("group_ms", C.c_double),
-                ("finish_ms", C.c_double), ("match_flops", C.c_double), ("match_pairs", C.c_double)]
+                ("finish_ms", C.c_double), ("match_flops", C.c_double), ("match_pairs", C.c_double),
+                ("tc_survivors", C.c_int64), ("tc_refs", C.c_int64), ("tc_max_error_ratio", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -107,7 +108,7 @@ class BatchItem(C.Structure):
 
 
 class BatchInfo(C.Structure):
-    _fields_ = [("match_parts", C.c_int), ("match_persistent", C.c_int), ("group_warps", C.c_int),
+    _fields_ = [("match_parts", C.c_int), ("match_persistent", C.c_int), ("match_form", C.c_int), ("group_warps", C.c_int),
                 ("group_ctas_per_sm", C.c_int), ("graphs", C.c_int), ("runs", C.c_int64), ("frames", C.c_int64),
                 ("kernel_launches", C.c_int64), ("graph_builds", C.c_int64), ("tunings", C.c_int64),
                 ("chunks", C.c_int), ("last_run_ms", C.c_double), ("arena_bytes", C.c_size_t)]
@@ -166,6 +167,7 @@ def lib():
                                             C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.nssb_bm3d_plane_stage_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                                     C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.nssb_bm3d_set_matcher.argtypes = [C.c_void_p, C.c_int]
         L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
         L.nssb_batch_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
@@ -307,6 +309,10 @@ class Node:
         st = KernelStats()
         check(lib().nssb_bm3d_stats(self.handle, int(enable_timing), int(reset), C.byref(st)))
         return st
+
+    def set_matcher(self, form: int) -> None:
+        """0: FP32 matcher (default); 1: tensor-core precision form (identical lists)."""
+        check(lib().nssb_bm3d_set_matcher(self.handle, int(form)))
 
     def frame_window(self, n: int):
         a, b = C.c_int(), C.c_int()

@@ -175,6 +175,15 @@ int nssb_match_spatial(const float* plane, int64_t stride, int width, int height
     });
 }
 
+int nssb_bm3d_set_matcher(nssb_bm3d* h, int form) {
+    return guarded([&] {
+        if (!h) throw std::invalid_argument("nssb_bm3d_set_matcher: invalid handle");
+        if (form != NSSB_MATCHER_FP32 && form != NSSB_MATCHER_TENSOR)
+            throw std::invalid_argument("nssb_bm3d_set_matcher: form must be NSSB_MATCHER_FP32 or NSSB_MATCHER_TENSOR");
+        h->engine->set_matcher(form);
+    });
+}
+
 int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int group,
                           int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats, void* stream) {
     int timeouts = 0;
@@ -272,7 +281,8 @@ int nssb_batch_create(int device_id, const nssb_arg* args, int nargs, nssb_batch
         for (int i = 0; i < nargs; ++i) {
             const nssb_arg& a = args[i];
             const std::string key = a.key ? a.key : "";
-            int* slot = key == "match_parts"         ? &opt.fixed.match.parts
+            int* slot = key == "match_form"          ? &opt.fixed.match.form
+                        : key == "match_parts"       ? &opt.fixed.match.parts
                         : key == "match_persistent"  ? &opt.fixed.match.persistent
                         : key == "group_warps"       ? &opt.fixed.group.warps
                         : key == "group_ctas_per_sm" ? &opt.fixed.group.ctas_per_sm
@@ -288,6 +298,8 @@ int nssb_batch_create(int device_id, const nssb_arg* args, int nargs, nssb_batch
             else *slot = (int)v;
         }
         const nssb::LaunchTunes& f = opt.fixed;
+        if (f.match.form != 0 && f.match.form != 1)
+            throw nssb::ArgumentError("nss_batch: match_form must be 0 or 1");
         if (f.match.parts != 1 && f.match.parts != 2 && f.match.parts != 4)
             throw nssb::ArgumentError("nss_batch: match_parts must be 1, 2 or 4");
         if (f.group.warps != 2 && f.group.warps != 4 && f.group.warps != 8)

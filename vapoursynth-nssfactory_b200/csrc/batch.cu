@@ -56,7 +56,8 @@ void EventClock::collect() {
 
 const std::vector<MatchTune>& match_candidates() {
     static const std::vector<MatchTune> c = {
-        {2, 0, nullptr}, {2, 1, nullptr}, {1, 0, nullptr}, {4, 0, nullptr}, {4, 1, nullptr}};
+        {2, 0, nullptr, 0, nullptr}, {2, 1, nullptr, 0, nullptr}, {1, 0, nullptr, 0, nullptr},
+        {4, 0, nullptr, 0, nullptr}, {4, 1, nullptr, 0, nullptr}, {2, 0, nullptr, 1, nullptr}};
     return c;
 }
 
@@ -209,7 +210,11 @@ void BatchPlan::layout(const BatchItem* items, int n, cudaStream_t stream) {
         arena_ = static_cast<char*>(dev_alloc(off));
         arena_cap_ = off;
     }
-    if (!queue_) queue_ = static_cast<int*>(dev_alloc(256));
+    if (!queue_) {
+        // bytes 0..3: the persistent matcher's tile counter; 64..: the tensor form's counters
+        queue_ = static_cast<int*>(dev_alloc(256));
+        NSSB_CUDA(cudaMemsetAsync(queue_, 0, 256, stream));
+    }
     arena_bytes_ = off;
     // num must start at zero; every finish leaves it zero again
     NSSB_CUDA(cudaMemsetAsync(arena_, 0, off, stream));
@@ -274,6 +279,7 @@ void BatchPlan::download(const BatchItem* items, int n, cudaStream_t s) {
 void BatchPlan::compute(cudaStream_t s, const LaunchTunes& tunes, StageClock& clock) {
     LaunchTunes t = tunes;
     t.match.queue = queue_;
+    t.match.tc = reinterpret_cast<TcCounters*>(queue_ + 16);
     for (int st = 0; st < 2; ++st) {
         for (const PreMatch& pm : prematch_[st]) {
             const Plane& pl = planes_[pm.plane];
@@ -291,7 +297,7 @@ void BatchPlan::compute(cudaStream_t s, const LaunchTunes& tunes, StageClock& cl
 
 namespace {
 bool same_tunes(const LaunchTunes& a, const LaunchTunes& b) {
-    return a.match.parts == b.match.parts && a.match.persistent == b.match.persistent &&
+    return a.match.parts == b.match.parts && a.match.persistent == b.match.persistent && a.match.form == b.match.form &&
            a.group.warps == b.group.warps && a.group.ctas_per_sm == b.group.ctas_per_sm;
 }
 }  // namespace
@@ -339,6 +345,7 @@ BatchEngine::BatchEngine(int device, const BatchOptions& opt) : device_(device),
     for (auto& e : t1_) NSSB_CUDA(cudaEventCreate(&e));
     info_.match_parts = opt_.fixed.match.parts;
     info_.match_persistent = opt_.fixed.match.persistent;
+    info_.match_form = opt_.fixed.match.form;
     info_.group_warps = opt_.fixed.group.warps;
     info_.group_ctas_per_sm = opt_.fixed.group.ctas_per_sm;
     info_.graphs = opt_.graphs ? 1 : 0;
@@ -485,6 +492,7 @@ void BatchEngine::run(const BatchItem* items, int n) {
     info_.chunks = (int)parts.size();
     info_.match_parts = last.match.parts;
     info_.match_persistent = last.match.persistent;
+    info_.match_form = last.match.form;
     info_.group_warps = last.group.warps;
     info_.group_ctas_per_sm = last.group.ctas_per_sm;
     info_.runs += 1;

@@ -205,8 +205,30 @@ void Engine::count_match(int w, int h, const StageParams& sp) {
     stats_.match_flops += pairs * 3.0 * sp.block * sp.block;
 }
 
+void Engine::set_matcher(int form) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (form == 1 && !tunes_.match.tc) {
+        auto* c = static_cast<TcCounters*>(dev_alloc(sizeof(TcCounters)));
+        allocations_.push_back(c);
+        NSSB_CUDA(cudaMemsetAsync(c, 0, sizeof(TcCounters), stream_));
+        tunes_.match.tc = c;
+    }
+    tunes_.match.form = form;
+}
+
 void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
     std::lock_guard<std::mutex> lock(mu_);
+    if (tunes_.match.tc) {
+        TcCounters c{};
+        NSSB_CUDA(cudaMemcpyAsync(&c, tunes_.match.tc, sizeof c, cudaMemcpyDeviceToHost, stream_));
+        NSSB_CUDA(cudaStreamSynchronize(stream_));
+        stats_.tc_survivors = (int64_t)c.survivors;
+        stats_.tc_refs = (int64_t)c.refs;
+        float r;
+        std::memcpy(&r, &c.max_ratio_bits, 4);
+        stats_.tc_max_error_ratio = r;
+        if (reset) NSSB_CUDA(cudaMemsetAsync(tunes_.match.tc, 0, sizeof(TcCounters), stream_));
+    }
     if (out) *out = stats_;
     if (reset) stats_ = nssb_kernel_stats{};
     timing_ = enable_timing != 0;

@@ -66,6 +66,10 @@ public:
     // and window caches included; host_frames: frames arrive in host memory).
     static size_t footprint(const Bm3dConfig& cfg, bool host_frames);
 
+    // 8x8 matcher form: 0 FP32, 1 tensor-core precision form (same lists).
+    void set_matcher(int form);
+    int matcher() const { return tunes_.match.form; }
+
     // Kernel accounting (nssb_bm3d_stats).
     void stats(int enable_timing, int reset, nssb_kernel_stats* out);
 

@@ -33,10 +33,13 @@ struct MatchBatch {
     MatchPlane p[kMaxBatchPlanes];
 };
 // Launch shape of the 8x8 matcher; every choice gives the same lists.
+struct TcCounters;
 struct MatchTune {
     int parts = 2;           // warp pairs splitting the window columns: 1, 2 or 4
     int persistent = 0;      // 1: one resident wave taking tiles from a device counter
     int* queue = nullptr;    // that counter (one int of device memory)
+    int form = 0;            // 0: FP32 SIMT matcher; 1: tensor-core distances + exact re-rank (same lists)
+    TcCounters* tc = nullptr;  // counters of the tensor form (device memory)
 };
 // The specialised exact matcher for 8x8 blocks (match8.cu) over a batch of
 // planes; false when the shape (bm_range, group, step) has no specialisation.

@@ -6,9 +6,9 @@
 // pixel split as hi = bf16(v), lo = bf16(v - hi): r.c ~ rh.ch + rh.cl + rl.ch,
 // three MMAs into one accumulator. With u = 2^-8, the split leaves
 // |r.c - that| <= ~3.1 u^2 S plus FP32 accumulation, S = sum |r_i c_i| <=
-// sqrt(|r|^2 |c|^2); the kernel takes E = 1.3e-3 sqrt(|r|^2 max|c|^2) +
-// 5e-5 (|r|^2 + max|c|^2) + 1e-5 |U| (about 4x the derived bound) as the
-// per-reference error margin. With U >= the K-th smallest approximate
+// sqrt(|r|^2 |c|^2), i.e. |d~ - d| <= 1.42e-4 S + (norm and final roundings);
+// the kernel takes E = 2.9e-4 sqrt(|r|^2 max|c|^2) + 1e-5 (|r|^2 + max|c|^2)
+// + 2e-6 |U| (twice the derived bound) as the per-reference error margin. With U >= the K-th smallest approximate
 // distance, every exact top-K candidate c has d~(c) <= U + 2E; those
 // "survivors" get the exact FP32 distance in this build's order (per-column
 // FMA chains, then the column tree) and the exact keys pick the group. A tile
@@ -58,7 +58,9 @@ struct Tc {
     static constexpr int NCS = DIST + kTcRefs * NW * 4;       // float [NC][128] candidate norms
     static constexpr int RS = NCS + NC * 128 * 4;             // float [RB][128] row sums of squares
     static constexpr int SURV = RS + RB * 128 * 4;            // uint16 [8 warps][NW] survivor indices
-    static constexpr int BYTES = SURV + 8 * NW * 2;
+    static constexpr int TP = 136;                            // FP32 tile pitch (>= 128 + 7)
+    static constexpr int TILE = SURV + 8 * NW * 2;            // float [RB][TP] the tile's pixels, exact
+    static constexpr int BYTES = TILE + RB * TP * 4;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -154,8 +156,7 @@ __device__ __forceinline__ float warp_min_f(float v) {
 }
 
 // Exact SSD in this build's order (per-column FMA chains, column tree).
-__device__ __forceinline__ float ssd8_exact(const float* __restrict__ a, int64_t sa, const float* __restrict__ b,
-                                            int64_t sb) {
+__device__ __forceinline__ float ssd8_exact(const float* a, int sa, const float* b, int sb) {
     float c[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) c[j] = 0.f;
@@ -163,7 +164,7 @@ __device__ __forceinline__ float ssd8_exact(const float* __restrict__ a, int64_t
     for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const float d = __fsub_rn(__ldg(a + i * sa + j), __ldg(b + i * sb + j));
+            const float d = __fsub_rn(a[i * sa + j], b[i * sb + j]);
             c[j] = __fmaf_rn(d, d, c[j]);
         }
     return column_tree<8>(c);
@@ -290,6 +291,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) match_tc_kernel(const __grid_co
                 bad |= !isfinite(v[q]);
             }
             rs[rr * 128 + m] = sq;
+            float* trow = reinterpret_cast<float*>(sm + T::TILE) + rr * T::TP;
+            trow[m] = v[0];
+            if (m >= 121) {  // the last 7 columns of the tile's row
+#pragma unroll
+                for (int q = 1; q < 8; ++q)
+                    if (m + q >= 128) trow[m + q] = v[q];
+            }
             uint32_t hi[4], lo[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) split2(v[2 * q], v[2 * q + 1], hi[q], lo[q]);
@@ -329,13 +337,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) match_tc_kernel(const __grid_co
     const uint32_t tmem = tmem_base;
     if (tid == 0) issue_row<R>(smem0, tmem, 0, &bars[0]);
     // candidate norms |c|^2 per (candidate row, column) while the first MMAs run
-    for (int e = tid; e < ncr * 128; e += kTcThreads) {
-        const int c = e >> 7, m = e & 127;
-        float s = 0.f;
+    {
+        float mx = 0.f;
+        for (int e = tid; e < ncr * 128; e += kTcThreads) {
+            const int c = e >> 7, m = e & 127;
+            float s = 0.f;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) s += rs[(c + i) * 128 + m];
-        ncs[e] = s;
-        if (X0 + m <= W - 8) atomicMax(&ncmax_bits, __float_as_uint(s));
+            for (int i = 0; i < 8; ++i) s += rs[(c + i) * 128 + m];
+            ncs[e] = s;
+            if (X0 + m <= W - 8) mx = fmaxf(mx, s);
+        }
+        mx = warp_max_ratio(mx);
+        if (lane == 0) atomicMax(&ncmax_bits, __float_as_uint(mx));
     }
     __syncthreads();
 
@@ -419,7 +432,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) match_tc_kernel(const __grid_co
             if (need <= 0) U = mv;
         }
         const float nr = nr_s[n];
-        const float E = 1.3e-3f * sqrtf(nr * ncmax) + 5e-5f * (nr + ncmax) + (U < kInf ? 1e-5f * fabsf(U) : 0.f);
+        const float E = 2.9e-4f * sqrtf(nr * ncmax) + 1e-5f * (nr + ncmax) + (U < kInf ? 2e-6f * fabsf(U) : 0.f);
         const float theta = U + 2.f * E;
         // survivors, compacted in window order
         int S = 0;
@@ -438,7 +451,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) match_tc_kernel(const __grid_co
         }
         __syncwarp();
         // exact distances of the survivors, exact keys
-        const float* refp = src + (int64_t)cy * ss + cxn;
+        const float* tile = reinterpret_cast<const float*>(sm + T::TILE);
+        const float* refp = tile + (cy - ylo) * T::TP + (cxn - X0);
         TcTop<K> top;
         top.init();
         float worst_ratio = 0.f;
@@ -446,7 +460,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) match_tc_kernel(const __grid_co
             const int q = surv[i];
             const int dy = q / NC, dx = q - dy * NC;
             const int xx = cxn - R + dx, yy = cy - R + dy;
-            const float de = ssd8_exact(refp, ss, src + (int64_t)yy * ss + xx, ss);
+            const float de = ssd8_exact(refp, T::TP, tile + (yy - ylo) * T::TP + (xx - X0), T::TP);
             top.add(tc_key(de, xx, yy));
             if (!flagged) worst_ratio = fmaxf(worst_ratio, fabsf(dn[q] - de) / E);
         }

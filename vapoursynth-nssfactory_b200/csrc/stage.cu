@@ -44,7 +44,9 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
         bool ok = false;
         if (sp.block == 8) {
             clock.begin(StageClock::kMatch);
-            ok = launch_match8_batch(mb, sp.bm_range, sp.group, stream, &tunes.match);
+            if (tunes.match.form == 1 && tunes.match.tc)
+                ok = launch_match_tc_batch(mb, sp.bm_range, sp.group, tunes.match.tc, stream);
+            if (!ok) ok = launch_match8_batch(mb, sp.bm_range, sp.group, stream, &tunes.match);
             clock.end(StageClock::kMatch);
         }
         if (!ok) {

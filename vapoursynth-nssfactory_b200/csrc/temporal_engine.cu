@@ -51,8 +51,10 @@ public:
 
     using Getter = std::function<void(int frame, const float* planes[3], int64_t strides[3])>;
 
-    TemporalStage(const Bm3dConfig& cfg, const StageParams* sp, bool wiener, cudaStream_t stream)
-        : cfg_(cfg), sp_(sp), wiener_(wiener), r_(cfg.radius), slots_(2 * cfg.radius + 1), stream_(stream) {
+    TemporalStage(const Bm3dConfig& cfg, const StageParams* sp, bool wiener, cudaStream_t stream,
+                  const MatchTune* tune)
+        : cfg_(cfg), sp_(sp), wiener_(wiener), r_(cfg.radius), slots_(2 * cfg.radius + 1), stream_(stream),
+          tune_(tune) {
         for (int p = 0; p < cfg_.planes; ++p) {
             const int w = cfg_.plane_w[p], h = cfg_.plane_h[p];
             pitch_[p] = (int64_t)((w + 31) / 32) * 32;
@@ -211,8 +213,17 @@ private:
                     tp.stride[t] = wiener_ ? rs[t][mp] : ss[t][mp];
                 }
                 const StageParams& ms = sp_[mp];
-                launch_match_spatial(tp.plane[r_], tp.stride[r_], cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
-                                     ms.step, ms.bm_range, ms.group, pos_[mp], dist_[mp], count_[mp], stream_);
+                bool tc = false;
+                if (tune_ && tune_->form == 1 && tune_->tc && ms.block == 8) {
+                    mbatch_.n = 1;
+                    mbatch_.step = ms.step;
+                    mbatch_.p[0] = MatchPlane{tp.plane[r_], tp.stride[r_], pos_[mp], dist_[mp], count_[mp],
+                                              cfg_.plane_w[mp], cfg_.plane_h[mp], 0, 0, 0};
+                    tc = launch_match_tc_batch(mbatch_, ms.bm_range, ms.group, tune_->tc, stream_);
+                }
+                if (!tc)
+                    launch_match_spatial(tp.plane[r_], tp.stride[r_], cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
+                                         ms.step, ms.bm_range, ms.group, pos_[mp], dist_[mp], count_[mp], stream_);
                 launch_match_temporal(tp, ntemp, r_, vbegin, vend, cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
                                       ms.step, ms.group, ms.ps_num, ms.ps_range, pos_[mp], slot_[mp], dist_[mp],
                                       count_[mp], stream_);
@@ -264,6 +275,8 @@ private:
     int next_c_ = 0;
     std::vector<void*> mem_;
     FinishBatch fbatch_;
+    const MatchTune* tune_;  // the engine's matcher form (read at each centre)
+    MatchBatch mbatch_;
 };
 
 // Device frames of the temporal window: host frames are uploaded once and kept
@@ -372,9 +385,9 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
     if (!plan_) {
         plan_.reset(new Plan());
         const bool wiener_final = cfg_.two_stage || cfg_.has_ref;
-        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_);
+        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_, &tunes_.match);
         if (cfg_.two_stage) {
-            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_);
+            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_, &tunes_.match);
             plan_->basic_cache = std::make_unique<FrameCache>(cfg_, 2 * r + 2, stream_);
         }
     }
