@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--served", type=int, default=2000, help="requests of the serving leg (0: skip it)")
+    ap.add_argument("--no-legs", action="store_true", help="skip the temporal (C3) and mixed-batch (C4) legs")
+    ap.add_argument("--c3-frames", type=int, default=60)
     ap.add_argument("--served-plain", type=int, default=300,
                     help="requests of the same stream rendered by the per-frame drop-in for comparison")
     return ap.parse_args()
@@ -326,6 +328,9 @@ def our_arm(args):
                                "note": "plain form, one pass over the step's frames"},
         "clocks": clock,
     }
+    if not args.no_legs:
+        out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
+        out["batched_c4"] = c4_leg(nssb, synth, dev)
     if args.served > 0:
         out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain))
         out["served"]["note"] = ("seeded Poisson arrivals at 200 req/s; latency = submission -> outputs in pinned "
@@ -346,6 +351,130 @@ def our_arm(args):
         print(json.dumps(out), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def c3_leg(nssb, synth, dev, frames_n, check_psnr):
+    """Temporal two-stage BM3D, radius 2, YUV420PS 1920x1080, sigma 10: the
+    panning sequence (textured background at 1-2 px/frame + 5 moving
+    rectangles). FP32 matcher vs the precision form (tensor-core distances +
+    exact re-rank) on the same device-resident frames, in order."""
+    import torch
+
+    frames = synth.panning_clip(3100, 1920, 1080, frames=frames_n, sigma=10.0)
+    d = [tuple(torch.from_numpy(p).to(dev) for p in f) for f in frames]
+    outs = {}
+    res = {"workload": f"temporal two-stage BM3D (final=1), radius 2, YUV420PS 1920x1080, sigma 10, "
+                       f"{frames_n} frames (panning background + 5 moving rectangles)"}
+    for form in (0, 1):
+        node = nssb.BM3D(nssb.Clip.from_frames(d, nssb.YUV, 1, 1), sigma=10.0, radius=2, final=1)
+        node.set_matcher(form)
+        o = [tuple(torch.empty_like(p) for p in f) for f in d]
+        for n in range(min(4, frames_n)):  # warm-up (kernels loaded, engine planned)
+            node.get_frame(n, out=o[n])
+        node.close()
+        node = nssb.BM3D(nssb.Clip.from_frames(d, nssb.YUV, 1, 1), sigma=10.0, radius=2, final=1)
+        node.set_matcher(form)
+        node.stats(True, True)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for n in range(frames_n):
+            node.get_frame(n, out=o[n])
+        e.record()
+        torch.cuda.synchronize()
+        st = node.stats(False, True)
+        key = "fp32" if form == 0 else "precision"
+        res[f"{key}_fps"] = frames_n / (s.elapsed_time(e) / 1e3)
+        res[f"{key}_kernel_ms"] = {"match": st.match_ms, "group": st.group_ms, "finish": st.finish_ms}
+        if form == 1:
+            res["precision_survivors_per_ref"] = st.tc_survivors / max(1, st.tc_refs)
+            res["precision_max_error_over_margin"] = st.tc_max_error_ratio
+        outs[form] = o
+        node.close()
+    same = all(torch.equal(a, b) for f0, f1 in zip(outs[0], outs[1]) for a, b in zip(f0, f1))
+    res["precision_equals_fp32_bitwise"] = bool(same)
+    res["group_index_agreement"] = 1.0 if same else None
+    if check_psnr:
+        # the CPU restatement on a 256x144 crop of the first 5 frames' luma (the oracle is slow at 1080p)
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        crop = [np.ascontiguousarray(f[0][200:344, 400:656]) for f in frames[:5]]
+        node = nssb.BM3D(nssb.Clip.from_frames([(c,) for c in crop], nssb.GRAY), sigma=10.0, radius=2, final=1)
+        node.set_matcher(1)
+        got = [node.get_frame(n)[0] for n in range(5)]
+        node.close()
+        st = O.stage(O.effective_sigma(10.0))
+        basic = O.bm3d_clip_plane(crop, st, 2)
+        want = O.bm3d_clip_plane(crop, st, 2, ref_frames=basic)
+        res["psnr_vs_cpu_db_min"] = float(min(O.psnr(g, w) for g, w in zip(got, want)))
+        res["psnr_sample"] = "256x144 luma crop of the first 5 frames, precision form vs the CPU restatement"
+    return res
+
+
+def c4_leg(nssb, synth, dev, seed=4000):
+    """64 frames of uneven sizes (16 x 854x480, 16 x 1280x720, 24 x 1920x1080,
+    8 x 3840x2160), each Gray or YUV420PS (seeded choice), sigma drawn from
+    {3, 5, 10, 20}, two-stage, radius 0: the per-frame drop-in vs one batched
+    call (autotuned, graph-replayed) on device-resident frames."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    sizes = [(854, 480)] * 16 + [(1280, 720)] * 16 + [(1920, 1080)] * 24 + [(3840, 2160)] * 8
+    nodes, reqs, outs = [], [], []
+    kinds = {"gray": 0, "yuv420": 0}
+    for i, (w, h) in enumerate(sizes):
+        sigma = float(rng.choice([3.0, 5.0, 10.0, 20.0]))
+        yuv = bool(rng.integers(2))
+        if yuv:
+            f = synth.yuv420_clip(seed + i, w, h, 1, sigma)[0]
+            clip = nssb.Clip.from_frames([tuple(torch.from_numpy(p).to(dev) for p in f)], nssb.YUV, 1, 1)
+        else:
+            f = (synth.gray_frame(seed + i, w, h, sigma)[0],)
+            clip = nssb.Clip.from_frames([tuple(torch.from_numpy(p).to(dev) for p in f)], nssb.GRAY)
+        kinds["yuv420" if yuv else "gray"] += 1
+        node = nssb.BM3D(clip, sigma=sigma, final=1)
+        nodes.append(node)
+        reqs.append((node, 0))
+        outs.append(tuple(torch.empty_like(p) for p in clip.frames[0]))
+    px = sum(sum(p.numel() for p in o) for o in outs)
+
+    def plain():
+        for (node, n), o in zip(reqs, outs):
+            node.get_frame(n, out=o)
+
+    batch = nssb.Batch()
+
+    def batched():
+        batch.run(reqs, outs=outs)
+
+    res = {"workload": "64 frames: 16 x 854x480, 16 x 1280x720, 24 x 1920x1080, 8 x 3840x2160; "
+                       f"{kinds['gray']} Gray / {kinds['yuv420']} YUV420PS (seeded); sigma from {{3,5,10,20}}; "
+                       "two-stage, radius 0", "megapixels_per_step": px / 1e6}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(3):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        res[f"{name}_fps"] = 3 * len(reqs) / (s.elapsed_time(e) / 1e3)
+        if name == "plain":
+            ref = [tuple(p.clone() for p in o) for o in outs]
+    res["batched_over_plain"] = res["batched_fps"] / res["plain_fps"]
+    res["batched_equals_plain_bitwise"] = bool(all(torch.equal(a, b) for ro, o in zip(ref, outs) for a, b in zip(ro, o)))
+    inf = batch.info()
+    res["batched_shape"] = {"match_form": inf.match_form, "match_parts": inf.match_parts,
+                            "match_persistent": inf.match_persistent, "group_warps": inf.group_warps,
+                            "group_ctas_per_sm": inf.group_ctas_per_sm, "kernels_per_step": int(inf.kernel_launches),
+                            "graph": bool(inf.graphs)}
+    batch.close()
+    for node in nodes:
+        node.close()
+    return res
 
 
 SERVED_RES = {"480p": (854, 480), "720p": (1280, 720), "1080p": (1920, 1080), "2160p": (3840, 2160)}
