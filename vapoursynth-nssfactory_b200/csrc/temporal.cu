@@ -190,10 +190,10 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
     count[job] = 1 + global.n;
 }
 
-// ---- fast path: 8x8 blocks, ps_num <= 8, ps_range <= 15 ----
+// ---- fast path: 8x8 blocks, ps_num <= 8, ps_range <= 12 ----
 //
-// A CTA is 4 references x 2 warps; warp 2w searches reference w's chain
-// towards earlier slots, warp 2w+1 towards later ones. In a layer the warp's
+// A warp per reference searches the chain towards earlier slots, then the one
+// towards later slots (4 references per CTA). In a layer the warp's
 // lanes take the (window, column) pairs of the union of the ps_num windows;
 // a lane streams the column's image rows from the read-only cache and applies
 // each row to the (up to 8) candidates that overlap it -- candidate k in
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
 // earlier window of the layer is skipped (the raster union's dedup). Each lane
 // keeps its PS best keys; the layer's ps_num best are drawn by warp minima
 // (keys are unique, so the result is the set's top, whatever the visit
-// order). The two chains' layer bests then merge with the spatial group.
+// order). The layer bests of both chains then merge with the spatial group.
 constexpr int kTRefs = 4;
 
 __device__ __forceinline__ uint64_t tk64(uint32_t d, uint32_t tyx) { return (uint64_t(d) << 32) | tyx; }
@@ -241,39 +241,130 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
     return v;
 }
 
-template <int PS>
-__global__ void __launch_bounds__(64 * kTRefs, 2)
+// One (window, column) task of a layer: the column's candidates (nk of them,
+// rows ya.. of window i) against the reference, in two passes over the
+// block's column halves; each finished, not-duplicated candidate enters the
+// lane's top list. NK > 0: nk == NK known at compile time (a full window),
+// every loop unrolled and the first-half sums kept in registers.
+template <int NK, int PS>
+__device__ __forceinline__ void temporal_column(const float* __restrict__ refp, int64_t rs,
+                                                const float* __restrict__ colp, int64_t ps, int nk, int x, int ya,
+                                                int i, const int (*cen)[2], int ps_range, int maxx, int maxy,
+                                                uint32_t tbits, LaneTop<PS>& top, float* h0s) {
+    constexpr int B = 8;
+    constexpr int NKS = NK > 0 ? NK : 32;
+    float h0r[NK > 0 ? NK : 1];
+    const float2 neg1 = make_float2(-1.f, -1.f);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float2 rf[B][2];
+#pragma unroll
+        for (int ii = 0; ii < B; ++ii) {
+            rf[ii][0] = make_float2(__ldg(refp + ii * rs + 4 * half), __ldg(refp + ii * rs + 4 * half + 1));
+            rf[ii][1] = make_float2(__ldg(refp + ii * rs + 4 * half + 2), __ldg(refp + ii * rs + 4 * half + 3));
+        }
+        float2 acc[8][2];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
+        auto emit = [&](int kd, float hs) {
+            if (half == 0) {
+                if constexpr (NK > 0) {
+#pragma unroll
+                    for (int q = 0; q < NKS; ++q)
+                        if (q == kd) h0r[q] = hs;
+                } else {
+                    h0s[kd] = hs;
+                }
+                return;
+            }
+            float first_half;
+            if constexpr (NK > 0) {
+                first_half = 0.f;
+#pragma unroll
+                for (int q = 0; q < NKS; ++q)
+                    if (q == kd) first_half = h0r[q];
+            } else {
+                first_half = h0s[kd];
+            }
+            const int y = ya + kd;
+            bool dup = false;
+            for (int j = 0; j < i; ++j) {
+                const int jx = cen[j][0], jy = cen[j][1];
+                dup |= x >= max(0, jx - ps_range) && x <= min(maxx, jx + ps_range) && y >= max(0, jy - ps_range) &&
+                       y <= min(maxy, jy + ps_range);
+            }
+            if (!dup) top.add(tk64(canon(__fadd_rn(first_half, hs)), tbits | (uint32_t(y) << 13) | uint32_t(x)));
+        };
+        auto row = [&](int s, int slot_base) {
+            // image row ya + s: its 4 columns of this half, applied to the candidates k = s - ii
+            const float* rowp = colp + (int64_t)s * ps + 4 * half;
+            const float2 p01 = make_float2(__ldg(rowp), __ldg(rowp + 1));
+            const float2 p23 = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
+#pragma unroll
+            for (int ii = 0; ii < B; ++ii) {
+                const int k = s - ii;
+                if (k >= 0 && k < (NK > 0 ? NK : nk)) {
+                    const int sl = (slot_base - ii) & 7;
+                    const float2 d01 = __ffma2_rn(p01, neg1, rf[ii][0]);
+                    const float2 d23 = __ffma2_rn(p23, neg1, rf[ii][1]);
+                    acc[sl][0] = __ffma2_rn(d01, d01, acc[sl][0]);
+                    acc[sl][1] = __ffma2_rn(d23, d23, acc[sl][1]);
+                }
+            }
+            const int kd = s - (B - 1);
+            if (kd >= 0 && kd < (NK > 0 ? NK : nk)) {
+                const int sl = (slot_base + 1) & 7;
+                const float2 a = acc[sl][0], b = acc[sl][1];
+                acc[sl][0] = acc[sl][1] = make_float2(0.f, 0.f);
+                emit(kd, __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y)));
+            }
+        };
+        if constexpr (NK > 0) {
+#pragma unroll
+            for (int s = 0; s < NK + B - 1; ++s) row(s, s);
+        } else {
+            for (int s0 = 0; s0 < nk + B - 1; s0 += 8) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (s0 + u < nk + B - 1) row(s0 + u, u);
+            }
+        }
+    }
+}
+
+// A warp per reference: the chain towards earlier slots, then the one
+// towards later slots, then the merge -- no block-level synchronisation.
+template <int PS, int PR>
+__global__ void __launch_bounds__(32 * kTRefs, 4)
     temporal8_kernel(TemporalPlanes tp, int ntemp, int t0, int first, int last, int W, int H, int G, int ps_num,
                      int ps_range, int jobs, int32_t* __restrict__ pos, int32_t* __restrict__ slot,
                      float* __restrict__ dist, int32_t* __restrict__ count) {
     constexpr int B = 8;
-    __shared__ int cen[kTRefs][2][8][2];                 // layer centres (x, y) per chain
-    __shared__ uint64_t chain_top[kTRefs][2][16 * 8];    // layer bests per chain (<= 16 layers x ps_num)
-    __shared__ int chain_n[kTRefs][2];
-    __shared__ float h0s[64 * kTRefs][27];               // per lane: first-half sums down a column (<= 25)
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r = warp >> 1, dir = warp & 1;
-    const int job = blockIdx.x * kTRefs + r;
-    const bool live = job < jobs;
-    int n = 0;
-    if (live) n = count[job];
+    __shared__ int cen[kTRefs][8][2];               // the layer's window centres (x, y)
+    __shared__ uint64_t tops[kTRefs][2 * 16 * 8];   // every layer's bests, both directions
+    __shared__ float h0s[32 * kTRefs][27];          // first-half sums (windows clamped by the image)
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int job = blockIdx.x * kTRefs + w;
+    if (job >= jobs) return;  // a whole warp
+    const int n = count[job];
     int32_t* op = pos + (int64_t)job * G;
-    const bool search = live && n > 0 && ntemp > 1 && G > 1 && first < last;
-    if (live && dir == 0)
-        for (int q = lane; q < G; q += 32) slot[(int64_t)job * G + q] = q < n ? t0 : -1;
-    int nchain = 0;
-    if (search) {
-        const int cx = pos_x(op[0]), cy = pos_y(op[0]);
-        const float* refp = tp.plane[t0] + (int64_t)cy * tp.stride[t0] + cx;
-        const int64_t rs = tp.stride[t0];
-        const int nseed = min(n, ps_num);
+    int32_t* os = slot + (int64_t)job * G;
+    for (int q = lane; q < G; q += 32) os[q] = q < n ? t0 : -1;
+    if (n <= 0 || ntemp == 1 || G == 1 || first >= last) return;
+    const int cx = pos_x(op[0]), cy = pos_y(op[0]);
+    const float* refp = tp.plane[t0] + (int64_t)cy * tp.stride[t0] + cx;
+    const int64_t rs = tp.stride[t0];
+    const int nseed = min(n, ps_num);
+    const int maxx = W - B, maxy = H - B, span = 2 * ps_range + 1;
+    int ntop = 0;
+    for (int dir = 0; dir < 2; ++dir) {
+        __syncwarp();
         if (lane < nseed) {
-            cen[r][dir][lane][0] = pos_x(op[lane]);
-            cen[r][dir][lane][1] = pos_y(op[lane]);
+            cen[w][lane][0] = pos_x(op[lane]);
+            cen[w][lane][1] = pos_y(op[lane]);
         }
         __syncwarp();
         int nc = nseed;
-        const int maxx = W - B, maxy = H - B, span = 2 * ps_range + 1;
         const int sign = dir == 0 ? -1 : 1;
         for (int dt = 1; dt <= (ntemp - 1) / 2; ++dt) {
             const int t = t0 + sign * dt;
@@ -284,69 +375,19 @@ __global__ void __launch_bounds__(64 * kTRefs, 2)
             top.init();
             for (int task = lane; task < nc * span; task += 32) {
                 const int i = task / span, col = task - i * span;
-                const int wcx = cen[r][dir][i][0], wcy = cen[r][dir][i][1];
+                const int wcx = cen[w][i][0], wcy = cen[w][i][1];
                 const int x = max(0, wcx - ps_range) + col;
                 if (x > min(maxx, wcx + ps_range)) continue;
                 const int ya = max(0, wcy - ps_range), yb = min(maxy, wcy + ps_range);
-                const int nk = yb - ya + 1;  // candidates down this column
-                float* h0 = h0s[threadIdx.x];  // first-half sums, one per candidate
+                const int nk = yb - ya + 1;
                 const float* colp = pl + (int64_t)ya * ps + x;
-#pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    float2 rf[B][2];
-#pragma unroll
-                    for (int ii = 0; ii < B; ++ii) {
-                        rf[ii][0] = make_float2(__ldg(refp + ii * rs + 4 * half), __ldg(refp + ii * rs + 4 * half + 1));
-                        rf[ii][1] = make_float2(__ldg(refp + ii * rs + 4 * half + 2),
-                                                __ldg(refp + ii * rs + 4 * half + 3));
-                    }
-                    float2 acc[8][2];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
-                    const float2 neg1 = make_float2(-1.f, -1.f);
-                    for (int s0 = 0; s0 < nk + B - 1; s0 += 8) {
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            const int s = s0 + u;  // image row ya + s
-                            if (s < nk + B - 1) {
-                                const float* rowp = colp + (int64_t)s * ps + 4 * half;
-                                const float2 p01 = make_float2(__ldg(rowp), __ldg(rowp + 1));
-                                const float2 p23 = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
-#pragma unroll
-                                for (int ii = 0; ii < B; ++ii) {
-                                    const int k = s - ii;
-                                    if (k >= 0 && k < nk) {
-                                        const float2 d01 = __ffma2_rn(p01, neg1, rf[ii][0]);
-                                        const float2 d23 = __ffma2_rn(p23, neg1, rf[ii][1]);
-                                        acc[(u - ii) & 7][0] = __ffma2_rn(d01, d01, acc[(u - ii) & 7][0]);
-                                        acc[(u - ii) & 7][1] = __ffma2_rn(d23, d23, acc[(u - ii) & 7][1]);
-                                    }
-                                }
-                                const int kd = s - (B - 1);  // candidate finished by this row
-                                if (kd >= 0 && kd < nk) {
-                                    const float2 a = acc[(u + 1) & 7][0], b = acc[(u + 1) & 7][1];
-                                    acc[(u + 1) & 7][0] = acc[(u + 1) & 7][1] = make_float2(0.f, 0.f);
-                                    const float hs = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
-                                    if (half == 0) {
-                                        h0[kd] = hs;
-                                    } else {
-                                        const float first_half = h0[kd];
-                                        const int y = ya + kd;
-                                        bool dup = false;
-                                        for (int j = 0; j < i; ++j) {
-                                            const int jx = cen[r][dir][j][0], jy = cen[r][dir][j][1];
-                                            dup |= x >= max(0, jx - ps_range) && x <= min(maxx, jx + ps_range) &&
-                                                   y >= max(0, jy - ps_range) && y <= min(maxy, jy + ps_range);
-                                        }
-                                        if (!dup)
-                                            top.add(tk64(canon(__fadd_rn(first_half, hs)),
-                                                         (uint32_t(t) << 26) | (uint32_t(y) << 13) | uint32_t(x)));
-                                    }
-                                }
-                            }
-                        }
-                    }
-                }
+                const uint32_t tbits = uint32_t(t) << 26;
+                if (PR > 0 && nk == 2 * PR + 1)
+                    temporal_column<2 * PR + 1, PS>(refp, rs, colp, ps, nk, x, ya, i, cen[w], ps_range, maxx, maxy,
+                                                    tbits, top, h0s[threadIdx.x]);
+                else
+                    temporal_column<0, PS>(refp, rs, colp, ps, nk, x, ya, i, cen[w], ps_range, maxx, maxy, tbits,
+                                           top, h0s[threadIdx.x]);
             }
             // the layer's ps_num best over the warp
             int got = 0;
@@ -354,27 +395,24 @@ __global__ void __launch_bounds__(64 * kTRefs, 2)
                 const uint64_t m = warp_min64(top.k[0]);
                 if (m == ~0ull) break;
                 if (top.k[0] == m) top.pop();
-                if (lane == 0) chain_top[r][dir][nchain + q] = m;
+                if (lane == 0) tops[w][ntop + q] = m;
                 ++got;
             }
             __syncwarp();
             if (lane < got) {
-                const uint64_t m = chain_top[r][dir][nchain + lane];
-                cen[r][dir][lane][0] = int(m & 0x1fff);
-                cen[r][dir][lane][1] = int((m >> 13) & 0x1fff);
+                const uint64_t m = tops[w][ntop + lane];
+                cen[w][lane][0] = int(m & 0x1fff);
+                cen[w][lane][1] = int((m >> 13) & 0x1fff);
             }
-            nchain += got;
+            ntop += got;
             nc = got;
             __syncwarp();
         }
     }
-    if (lane == 0) chain_n[r][dir] = nchain;
-    __syncthreads();
-    if (!search || dir != 0 || lane != 0) return;
+    if (lane != 0) return;
     // the global group: the spatial matches (self excluded) and both chains' layer bests
     float* od = dist + (int64_t)job * G;
-    int32_t* os = slot + (int64_t)job * G;
-    uint64_t best[64];
+    uint64_t best[64] = {};
     int nb = 0;
     auto push = [&](uint64_t v) {
         if (nb > 0 && nb == G - 1 && !(v < best[nb - 1])) return;
@@ -387,8 +425,7 @@ __global__ void __launch_bounds__(64 * kTRefs, 2)
     };
     for (int i = 1; i < n; ++i)
         push(tk64(canon(od[i]), (uint32_t(t0) << 26) | (uint32_t(pos_y(op[i])) << 13) | uint32_t(pos_x(op[i]))));
-    for (int c = 0; c < 2; ++c)
-        for (int i = 0; i < chain_n[r][c]; ++i) push(chain_top[r][c][i]);
+    for (int i = 0; i < ntop; ++i) push(tops[w][i]);
     for (int q = 0; q < G - 1; ++q) {
         const bool valid = q < nb;
         const uint64_t k = valid ? best[q] : 0;
@@ -413,17 +450,17 @@ void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int 
     const int first = valid_begin < 0 ? 0 : valid_begin;
     const int last = valid_end < 0 ? ntemp : (valid_end < ntemp ? valid_end : ntemp);
     const int layers = (ntemp - 1) / 2;
-    if (block == 8 && ps_num <= 8 && ps_range <= 12 && group <= 64 && layers * ps_num <= 16 * 8 && ntemp <= 33) {
+    if (block == 8 && ps_num <= 8 && ps_range <= 12 && group <= 64 && 2 * layers * ps_num <= 2 * 16 * 8 &&
+        ntemp <= 33) {
         const dim3 g8(ceil_div(jobs, kTRefs));
-        if (ps_num <= 2)
-            temporal8_kernel<2><<<g8, 64 * kTRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, group,
-                                                               ps_num, ps_range, jobs, pos, slot, dist, count);
-        else if (ps_num <= 4)
-            temporal8_kernel<4><<<g8, 64 * kTRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, group,
-                                                               ps_num, ps_range, jobs, pos, slot, dist, count);
-        else
-            temporal8_kernel<8><<<g8, 64 * kTRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, group,
-                                                               ps_num, ps_range, jobs, pos, slot, dist, count);
+        auto go = [&](auto kern) {
+            kern<<<g8, 32 * kTRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, group, ps_num,
+                                                 ps_range, jobs, pos, slot, dist, count);
+        };
+        const bool r4 = ps_range == 4;
+        if (ps_num <= 2) r4 ? go(temporal8_kernel<2, 4>) : go(temporal8_kernel<2, 0>);
+        else if (ps_num <= 4) r4 ? go(temporal8_kernel<4, 4>) : go(temporal8_kernel<4, 0>);
+        else r4 ? go(temporal8_kernel<8, 4>) : go(temporal8_kernel<8, 0>);
         NSSB_CUDA(cudaGetLastError());
         return;
     }
