@@ -70,6 +70,18 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(values, pg, device):
+    """Element-wise maximum over the ranks of the process group (timings:
+    the slowest rank sets the job's time); the values themselves with no group."""
+    if pg is None:
+        return list(values)
+    import torch
+
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -283,10 +295,7 @@ def our_arm(args):
     barrier()
     hinfo = batch.info()
 
-    if pg is not None:
-        t = torch.tensor([dev_ms, e2e_s, plain_ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms, e2e_s, plain_ms = float(t[0]), float(t[1]), float(t[2])
+    dev_ms, e2e_s, plain_ms = max_over_ranks([dev_ms, e2e_s, plain_ms], pg, dev)
 
     value = world * nf * args.steps / (dev_ms / 1e3)
     plain_value = world * nf * args.steps / (plain_ms / 1e3)
