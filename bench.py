@@ -345,6 +345,7 @@ def our_arm(args):
         out["served"]["note"] = ("seeded Poisson arrivals at 200 req/s; latency = submission -> outputs in pinned "
                                  "host memory; per rank")
     if rank == 0 and world == 1 and not args.no_cpu:
+        out["accuracy"] = accuracy_leg(nssb, frames[0], dev)
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
 
@@ -360,6 +361,43 @@ def our_arm(args):
         print(json.dumps(out), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def accuracy_leg(nssb, frame, dev):
+    """Stage errors against an FP64 host recomputation of the same groups, and
+    the near-tie rate of the matcher against the reference's own SSD order, on
+    the luma plane of one workload frame."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    y = np.ascontiguousarray(frame[0])
+    h, w = y.shape
+    st = O.stage(O.effective_sigma(SIGMA))
+    src = torch.from_numpy(y).to(dev)
+    basic = torch.empty_like(src)
+    final = torch.empty_like(src)
+    L = nssb.lib()
+    for dst, ref in ((basic, None), (final, basic)):
+        nssb.check(L.nssb_bm3d_plane_stage(src.data_ptr(), ref.data_ptr() if ref is not None else None,
+                                           dst.data_ptr(), w, w, h, st.sigma, 8, 8, 8, 9, None))
+    torch.cuda.synchronize()
+    b, f = basic.cpu().numpy(), final.cpu().numpy()
+    b64 = O.bm3d_plane_f64(y, st)
+    f64 = O.bm3d_plane_f64(y, st, ref=b)
+    bad, refs = O.order_mismatch(y, st)
+
+    def err(a, r):
+        d = a.astype(np.float64) - r
+        return {"max_abs": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d)))}
+
+    return {"plane": f"luma {w}x{h} of the first workload frame",
+            "basic_stage_vs_fp64": err(b, b64), "final_stage_vs_fp64": err(f, f64),
+            "near_tie_groups_vs_reference_order": {"refs": refs, "differing": bad, "rate": bad / max(1, refs)},
+            "note": "FP64 recomputation on the FP32 matcher's groups (the final stage on the device's basic "
+                    "estimate); the tie rate compares this build's SSD order with the reference's 8-lane "
+                    "AVX2 order on the CPU"}
 
 
 def c3_leg(nssb, synth, dev, frames_n, check_psnr):

@@ -922,3 +922,80 @@ int om_bm3d_frames_mt(const float* const* src, float* const* dst, float* const* 
     for (int i = 0; i < started; ++i) pthread_join(tid[i], NULL);
     return j.failed ? -1 : 0;
 }
+
+/* One radius-0 stage of one plane with the group filter and the sums in
+ * FP64: the groups are those of the FP32 matcher (matched on ref for Wiener,
+ * else on src), so the result isolates the arithmetic error of a stage. */
+int om_bm3d_plane_f64(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width, int height,
+                      const om_stage* st, int wiener, double* dst, ptrdiff_t dstride) {
+    if (st->sigma == 0.f) {
+        for (int y = 0; y < height; ++y)
+            for (int x = 0; x < width; ++x) dst[y * dstride + x] = src[y * sstride + x];
+        return 0;
+    }
+    const int block = st->block, group = st->group, area = block * block;
+    if (width < block || height < block) return -1;
+    const size_t plane = (size_t)width * (size_t)height;
+    double* num = (double*)calloc(plane * 2, sizeof(double));
+    double* cube = (double*)malloc((size_t)group * area * 2 * sizeof(double));
+    if (!num || !cube) {
+        free(num);
+        free(cube);
+        return -1;
+    }
+    double* den = num + plane;
+    double* rcube = cube + (size_t)group * area;
+    const float* ms = wiener ? ref : src;
+    const ptrdiff_t mst = wiener ? rstride : sstride;
+    const int nx = om_grid_count(width, block, st->step), ny = om_grid_count(height, block, st->step);
+    om_match m[OM_MAX_GROUP];
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int bx = om_grid_pos(i, width, block, st->step), by = om_grid_pos(j, height, block, st->step);
+            const int k = om_spatial_match(ms, mst, width, height, bx, by, block, st->bm_range, group, m, 0);
+            memset(cube, 0, (size_t)group * area * 2 * sizeof(double));
+            for (int q = 0; q < k; ++q)
+                for (int y = 0; y < block; ++y)
+                    for (int x = 0; x < block; ++x) {
+                        cube[(size_t)q * area + y * block + x] = src[(m[q].y + y) * sstride + m[q].x + x];
+                        if (wiener) rcube[(size_t)q * area + y * block + x] = ref[(m[q].y + y) * rstride + m[q].x + x];
+                    }
+            const double w = om_filter_group_f64(cube, wiener ? rcube : NULL, group, block, (double)st->sigma, wiener);
+            for (int q = 0; q < k; ++q)
+                for (int y = 0; y < block; ++y)
+                    for (int x = 0; x < block; ++x) {
+                        const size_t at = (size_t)(m[q].y + y) * width + m[q].x + x;
+                        num[at] += w * cube[(size_t)q * area + y * block + x];
+                        den[at] += w;
+                    }
+        }
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            const double d = den[(size_t)y * width + x];
+            dst[y * dstride + x] = d > 1e-12 ? num[(size_t)y * width + x] / d : src[y * sstride + x];
+        }
+    free(num);
+    free(cube);
+    return 0;
+}
+
+/* References of a plane whose groups differ between this build's SSD order
+ * and the reference's 8-lane AVX2 order (om_ssd_lanes8): the near-tie rate of
+ * the FP32 matcher against the reference CPU plugin's own rounding. */
+long om_order_mismatch(const float* plane, ptrdiff_t stride, int width, int height, const om_stage* st, long* refs) {
+    const int block = st->block;
+    const int nx = om_grid_count(width, block, st->step), ny = om_grid_count(height, block, st->step);
+    om_match a[OM_MAX_GROUP], b[OM_MAX_GROUP];
+    long bad = 0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int bx = om_grid_pos(i, width, block, st->step), by = om_grid_pos(j, height, block, st->step);
+            const int ka = om_spatial_match(plane, stride, width, height, bx, by, block, st->bm_range, st->group, a, 0);
+            const int kb = om_spatial_match(plane, stride, width, height, bx, by, block, st->bm_range, st->group, b, 1);
+            int same = ka == kb;
+            for (int q = 0; same && q < ka; ++q) same = a[q].x == b[q].x && a[q].y == b[q].y;
+            bad += !same;
+        }
+    if (refs) *refs = (long)nx * ny;
+    return bad;
+}

@@ -87,6 +87,13 @@ float om_haar_scale(int n, int j);
 float om_filter_group(float* cube, const float* ref, int group, int block, float sigma, int wiener);
 /* The same in double precision with exact cosines: the FP64 recomputation. */
 double om_filter_group_f64(double* cube, const double* ref, int group, int block, double sigma, int wiener);
+/* One radius-0 stage with the group filter and sums in FP64 on the FP32
+ * matcher's groups (matched on ref when wiener, else on src). */
+int om_bm3d_plane_f64(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width, int height,
+                      const om_stage* st, int wiener, double* dst, ptrdiff_t dstride);
+/* References whose groups differ between this build's SSD order and the
+ * reference's 8-lane AVX2 order; *refs receives the reference count. */
+long om_order_mismatch(const float* plane, ptrdiff_t stride, int width, int height, const om_stage* st, long* refs);
 
 /* ---- plane passes ---- */
 /* One stage of one plane at radius 0: match on ref (when wiener) or src,

@@ -48,6 +48,10 @@ def lib():
         fp = C.POINTER(C.c_float)
         L.om_ssd.restype = C.c_float
         L.om_ssd.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int]
+        L.om_bm3d_plane_f64.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int, C.POINTER(Stage), C.c_int,
+                                        C.POINTER(C.c_double), C.c_ssize_t]
+        L.om_order_mismatch.restype = C.c_long
+        L.om_order_mismatch.argtypes = [fp, C.c_ssize_t, C.c_int, C.c_int, C.POINTER(Stage), C.POINTER(C.c_long)]
         L.om_ssd_lanes8.restype = C.c_float
         L.om_ssd_lanes8.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t]
         L.om_spatial_match.restype = C.c_int
@@ -179,6 +183,30 @@ def bm3d_plane(src, st: Stage, ref=None, want_matches=False):
     if want_matches:
         return dst, matches, counts
     return dst
+
+
+def bm3d_plane_f64(src, st: Stage, ref=None) -> np.ndarray:
+    """One radius-0 stage, group filter and sums in FP64, on the FP32 matcher's
+    groups (matched on ref for the Wiener stage)."""
+    s = _f32(src)
+    h, w = s.shape
+    r = _f32(ref) if ref is not None else None
+    dst = np.empty((h, w), np.float64)
+    rc = lib().om_bm3d_plane_f64(_fp(s), w, _fp(r) if r is not None else None, w, w, h, C.byref(st),
+                                 int(r is not None), dst.ctypes.data_as(C.POINTER(C.c_double)), w)
+    if rc != 0:
+        raise RuntimeError("oracle FP64 plane pass failed")
+    return dst
+
+
+def order_mismatch(plane, st: Stage):
+    """(references whose groups differ between this build's SSD order and the
+    reference's AVX2 order, references)."""
+    p = _f32(plane)
+    h, w = p.shape
+    refs = C.c_long()
+    bad = lib().om_order_mismatch(_fp(p), w, w, h, C.byref(st), C.byref(refs))
+    return int(bad), int(refs.value)
 
 
 def bm3d_planes_chroma(planes, stages, refs=None):

@@ -177,3 +177,23 @@ def test_frame_api_chroma(nssb, oracle, synth, dev):
     want = oracle.bm3d_planes_chroma([y, u, v], stages, refs=basic)
     for c in range(3):
         assert oracle.psnr(both[c], want[c]) >= MIN_PSNR
+
+
+def test_stage_errors_vs_fp64(nssb, oracle, dev):
+    """Each stage against an FP64 host recomputation of the same groups."""
+    import importlib
+
+    synth = importlib.import_module("vapoursynth-nssfactory_b200.synth")
+    img = synth.gray_frame(33, 200, 136, 10)[0]
+    h, w = img.shape
+    st = oracle.stage(oracle.effective_sigma(10.0))
+    src = torch.from_numpy(img).to(dev)
+    basic, final = torch.empty_like(src), torch.empty_like(src)
+    for dst, ref in ((basic, None), (final, basic)):
+        nssb.check(nssb.lib().nssb_bm3d_plane_stage(src.data_ptr(), ref.data_ptr() if ref is not None else None,
+                                                    dst.data_ptr(), w, w, h, st.sigma, 8, 8, 8, 9, None))
+    torch.cuda.synchronize()
+    b, f = basic.cpu().numpy(), final.cpu().numpy()
+    for got, want in ((b, oracle.bm3d_plane_f64(img, st)), (f, oracle.bm3d_plane_f64(img, st, ref=b))):
+        d = got.astype(np.float64) - want
+        assert np.abs(d).max() < 1e-4 and np.sqrt(np.mean(d * d)) < 1e-5

@@ -326,3 +326,28 @@ def test_oracle_selection_equals_reference_header(oracle):
         cfg = (C.c_int * 9)(b, 8, g, r, rad, psn, psr, vb, ve)
         n = R.ref_predictive_match(arr, st, T, w, h, bx, by, t0, cfg, out)
         assert a == [(m.x, m.y, m.t, m.dist, m.ordinal) for m in out[:n]]
+
+
+def test_fp64_stage_agrees_with_fp32_oracle(oracle):
+    import importlib
+
+    synth = importlib.import_module("vapoursynth-nssfactory_b200.synth")
+    img = synth.gray_frame(31, 96, 72, 10)[0]
+    st = oracle.stage(oracle.effective_sigma(10.0))
+    ht = oracle.bm3d_plane(img, st)
+    ht64 = oracle.bm3d_plane_f64(img, st)
+    assert oracle.psnr(ht, ht64.astype(np.float32)) >= 110.0
+    wi = oracle.bm3d_plane(img, st, ref=ht)
+    wi64 = oracle.bm3d_plane_f64(img, st, ref=ht)
+    assert oracle.psnr(wi, wi64.astype(np.float32)) >= 110.0
+
+
+def test_order_mismatch_rate_is_small(oracle):
+    import importlib
+
+    synth = importlib.import_module("vapoursynth-nssfactory_b200.synth")
+    img = synth.gray_frame(32, 160, 120, 5)[0]
+    bad, refs = oracle.order_mismatch(img, oracle.stage(oracle.effective_sigma(5.0)))
+    assert refs == 20 * 15 and bad / refs < 0.05
+    flat = np.full((64, 64), 0.5, np.float32)  # exact ties everywhere: both orders sum zeros
+    assert oracle.order_mismatch(flat, oracle.stage(oracle.effective_sigma(5.0)))[0] == 0
