@@ -197,3 +197,19 @@ def test_stage_errors_vs_fp64(nssb, oracle, dev):
     for got, want in ((b, oracle.bm3d_plane_f64(img, st)), (f, oracle.bm3d_plane_f64(img, st, ref=b))):
         d = got.astype(np.float64) - want
         assert np.abs(d).max() < 1e-4 and np.sqrt(np.mean(d * d)) < 1e-5
+
+
+def test_memory_limit_fits_or_fails_at_creation(nssb, dev):
+    """memory_limit_mb is a creation error when the plan does not fit, and never changes the output."""
+    import importlib
+
+    synth = importlib.import_module("vapoursynth-nssfactory_b200.synth")
+    frames = [(synth.gray_frame(40 + i, 256, 160, 10)[0],) for i in range(3)]
+    clip = nssb.Clip.from_frames(frames, nssb.GRAY)
+    with pytest.raises(nssb.Error, match=r"nss_cuda.BM3D: memory_limit_mb is too small for this clip: each of the 1 "
+                                         r"stream\(s\) needs at least \d+ MiB"):
+        nssb.BM3D(clip, sigma=10, radius=1, final=1, memory_limit_mb=1)
+    a = nssb.BM3D(clip, sigma=10, final=1)
+    b = nssb.BM3D(clip, sigma=10, final=1, memory_limit_mb=4096)
+    for n in range(3):
+        assert np.array_equal(a.get_frame(n)[0], b.get_frame(n)[0])

@@ -126,6 +126,16 @@ int nssb_bm3d_create(const nssb_video_info* clip, const nssb_video_info* ref, co
         const nssb::Bm3dConfig cfg = nssb::parse_bm3d_call(*clip, ref, args, nargs);
         acquire_device(cfg.device_id, "nss_cuda.BM3D");
         auto h = std::make_unique<nssb_bm3d>();
+        // the memory plan (plan_planes, group_driver.cpp:571-600): a creation error
+        // when the filter's device memory cannot fit memory_limit_mb; this engine
+        // keeps whole planes resident, so it fits or it fails -- the limit never
+        // changes the output
+        if (cfg.memory_limit_mb > 0) {
+            const size_t need = nssb::Engine::footprint(cfg, true);
+            if (need > (size_t)cfg.memory_limit_mb << 20)
+                throw nssb::ArgumentError("nss_cuda.BM3D: memory_limit_mb is too small for this clip: each of the 1 "
+                                          "stream(s) needs at least " + std::to_string((need >> 20) + 1) + " MiB");
+        }
         h->engine = std::make_unique<nssb::Engine>(cfg);
         *out = h.release();
     });

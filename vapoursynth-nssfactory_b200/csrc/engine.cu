@@ -306,6 +306,7 @@ void Engine::get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int
     if (cfg_.has_ref && !ref) throw std::invalid_argument("nss_cuda.BM3D: ref frames missing");
     if (cfg_.radius > 0) {
         temporal_frame(n, clip, ref, first, count, memory, out);
+        collect_timing();
         return;
     }
     spatial_frame(n, clip, ref, first, memory);

@@ -123,6 +123,7 @@ private:
     StageScratch scratch_[3];
     std::unique_ptr<StageTables> tables_;
     LaunchTunes tunes_;
+    Clock clock_{this};
     std::vector<void*> allocations_;
     struct PlanDeleter {
         void operator()(Plan* p) const;

@@ -82,6 +82,10 @@ __global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restri
 // by exactly one thread), so the next stage finds it zero.
 constexpr int kFX = 64, kFY = 32, kFT = 256;
 
+// BT > 0: the block size known at compile time (8, the default), so the
+// halo tile's loads are a fixed, fully unrolled set issued before any of them
+// is stored; BT = 0: any block size.
+template <int BT>
 __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant__ FinishBatch fb) {
     extern __shared__ long long fsm[];  // wt[(kFY + B - 1)][(kFX + B - 1)], then hs[(kFY + B - 1)][kFX]
     int pl = 0;
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
         pl = lo;
     }
     const FinishPlane& P = fb.p[pl];
-    const int B = fb.block;
+    const int B = BT > 0 ? BT : fb.block;
     const int local = blockIdx.x - P.cta0;
     const int ty = local / P.tiles_x, tx = local - ty * P.tiles_x;
     const int x0 = tx * kFX, y0 = ty * kFY;
@@ -115,10 +119,29 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
     long long* hsp = fsm + rows * cols;
 #define wt(r, cc) wtp[(r) * cols + (cc)]
 #define hs(r, cc) hsp[(r) * kFX + (cc)]
-    for (int i = threadIdx.x; i < rows * cols; i += kFT) {
-        const int r = i / cols, cc = i - r * cols;
-        const int yy = y0 - B + 1 + r, xx = x0 - B + 1 + cc;
-        wt(r, cc) = (yy >= 0 && yy < P.H && xx >= 0 && xx < P.W) ? P.wsum[(int64_t)yy * P.acc_stride + xx] : 0ll;
+    if constexpr (BT > 0) {
+        constexpr int kRows = kFY + BT - 1, kCols = kFX + BT - 1, kN = (kRows * kCols + kFT - 1) / kFT;
+        long long v[kN];
+#pragma unroll
+        for (int t = 0; t < kN; ++t) {
+            const int i = threadIdx.x + t * kFT;
+            const int r = i / kCols, cc = i - r * kCols;
+            const int yy = y0 - BT + 1 + r, xx = x0 - BT + 1 + cc;
+            v[t] = (i < kRows * kCols && yy >= 0 && yy < P.H && xx >= 0 && xx < P.W)
+                       ? P.wsum[(int64_t)yy * P.acc_stride + xx]
+                       : 0ll;
+        }
+#pragma unroll
+        for (int t = 0; t < kN; ++t) {
+            const int i = threadIdx.x + t * kFT;
+            if (i < kRows * kCols) wtp[i] = v[t];
+        }
+    } else {
+        for (int i = threadIdx.x; i < rows * cols; i += kFT) {
+            const int r = i / cols, cc = i - r * cols;
+            const int yy = y0 - B + 1 + r, xx = x0 - B + 1 + cc;
+            wt(r, cc) = (yy >= 0 && yy < P.H && xx >= 0 && xx < P.W) ? P.wsum[(int64_t)yy * P.acc_stride + xx] : 0ll;
+        }
     }
     __syncthreads();
     // row sums: 8 consecutive columns of one row per task, sliding
@@ -156,8 +179,9 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
 void launch_finish_batch(const FinishBatch& fb, cudaStream_t stream) {
     if (fb.total_ctas <= 0) return;
     const size_t smem = (size_t)(kFY + fb.block - 1) * (kFX + fb.block - 1 + kFX) * sizeof(long long);
-    NSSB_CUDA(cudaFuncSetAttribute(finish_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    finish_batch_kernel<<<fb.total_ctas, kFT, smem, stream>>>(fb);
+    auto kern = fb.block == 8 ? finish_batch_kernel<8> : finish_batch_kernel<0>;
+    NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<fb.total_ctas, kFT, smem, stream>>>(fb);
     NSSB_CUDA(cudaGetLastError());
 }
 

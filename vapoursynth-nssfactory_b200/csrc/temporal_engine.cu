@@ -52,9 +52,9 @@ public:
     using Getter = std::function<void(int frame, const float* planes[3], int64_t strides[3])>;
 
     TemporalStage(const Bm3dConfig& cfg, const StageParams* sp, bool wiener, cudaStream_t stream,
-                  const MatchTune* tune)
+                  const MatchTune* tune, StageClock* clock)
         : cfg_(cfg), sp_(sp), wiener_(wiener), r_(cfg.radius), slots_(2 * cfg.radius + 1), stream_(stream),
-          tune_(tune) {
+          tune_(tune), clock_(clock) {
         for (int p = 0; p < cfg_.planes; ++p) {
             const int w = cfg_.plane_w[p], h = cfg_.plane_h[p];
             pitch_[p] = (int64_t)((w + 31) / 32) * 32;
@@ -105,7 +105,9 @@ public:
                 continue;
             }
             if (fb.n > 0 && sp_[p].block != fb.block) {
+                clock_->begin(StageClock::kFinish);
                 launch_finish_batch(fb, stream_);
+                clock_->end(StageClock::kFinish);
                 fb.n = 0;
                 fb.total_ctas = 0;
             }
@@ -115,7 +117,11 @@ public:
                                        finish_tiles_x(w), fb.total_ctas};
             fb.total_ctas += finish_tiles(w, h);
         }
-        if (fb.n > 0) launch_finish_batch(fb, stream_);
+        if (fb.n > 0) {
+            clock_->begin(StageClock::kFinish);
+            launch_finish_batch(fb, stream_);
+            clock_->end(StageClock::kFinish);
+        }
         finished_[sl] = true;
     }
 
@@ -213,6 +219,8 @@ private:
                     tp.stride[t] = wiener_ ? rs[t][mp] : ss[t][mp];
                 }
                 const StageParams& ms = sp_[mp];
+                clock_->count_match(cfg_.plane_w[mp], cfg_.plane_h[mp], ms);
+                clock_->begin(StageClock::kMatch);
                 bool tc = false;
                 if (tune_ && tune_->form == 1 && tune_->tc && ms.block == 8) {
                     mbatch_.n = 1;
@@ -227,6 +235,7 @@ private:
                 launch_match_temporal(tp, ntemp, r_, vbegin, vend, cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
                                       ms.step, ms.group, ms.ps_num, ms.ps_range, pos_[mp], slot_[mp], dist_[mp],
                                       count_[mp], stream_);
+                clock_->end(StageClock::kMatch);
                 matched0 = true;
             }
             GroupIO io{};
@@ -245,8 +254,10 @@ private:
             io.ref_stride = rstride;
             io.acc_stride = pitch_[p];
             const int jobs = grid_count(w, st.block, st.step) * grid_count(h, st.block, st.step);
+            clock_->begin(StageClock::kGroup);
             launch_group_filter(io, w, h, pos_[mp], slot_[mp], count_[mp], jobs, st.block, st.group, st.sigma,
                                 wiener_, cube_[p], cube_floats_[p], stream_);
+            clock_->end(StageClock::kGroup);
         }
         if (!legacy) {
             for (int m = std::max(0, c - r_); m <= std::min(N - 1, c + r_); ++m) {
@@ -276,6 +287,7 @@ private:
     std::vector<void*> mem_;
     FinishBatch fbatch_;
     const MatchTune* tune_;  // the engine's matcher form (read at each centre)
+    StageClock* clock_;      // the engine's launch accounting
     MatchBatch mbatch_;
 };
 
@@ -385,9 +397,9 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
     if (!plan_) {
         plan_.reset(new Plan());
         const bool wiener_final = cfg_.two_stage || cfg_.has_ref;
-        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_, &tunes_.match);
+        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_, &tunes_.match, &clock_);
         if (cfg_.two_stage) {
-            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_, &tunes_.match);
+            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_, &tunes_.match, &clock_);
             plan_->basic_cache = std::make_unique<FrameCache>(cfg_, 2 * r + 2, stream_);
         }
     }
