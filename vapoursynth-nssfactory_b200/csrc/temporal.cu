@@ -438,6 +438,159 @@ __global__ void __launch_bounds__(32 * kTRefs, 4)
     count[job] = 1 + nb;
 }
 
+// ---- streaming form: 8x8 blocks, ps_range PR, ps_num PS (1 or 2) ----
+//
+// The spatial matcher's schedule applied to the temporal layers: two lanes
+// per reference (block columns 0-3 and 4-7, each half of the reference in
+// registers for the whole search), 16 references per warp, so every lane
+// works on its own reference's windows. A lane walks each window of the layer
+// column by column; the column's image rows stream through and each row is
+// applied to the candidates overlapping it (slot k & 7); a finished
+// candidate's halves meet through one shuffle. Every loop has a trip count
+// shared by the warp (windows clipped by the image predicate their missing
+// rows and columns off), so the shuffles stay converged. Both lanes of a
+// reference keep identical lists: the layer's PS best, and the group itself
+// (spatial matches, then every layer's best, inserted as they are found --
+// the same set, hence the same top, as the reference's merge).
+constexpr int kSRefs = 64;  // references per CTA (4 warps)
+
+template <int K, int PS, int PR>
+__global__ void __launch_bounds__(2 * kSRefs, 4)
+    temporal8s_kernel(TemporalPlanes tp, int ntemp, int t0, int first, int last, int W, int H, int ps_num,
+                      int jobs, int32_t* __restrict__ pos, int32_t* __restrict__ slot, float* __restrict__ dist,
+                      int32_t* __restrict__ count) {
+    constexpr int B = 8, G = K + 1, SPAN = 2 * PR + 1, ROWS = SPAN + B - 1;
+    const int lane = threadIdx.x & 31, half = lane >> 4;
+    const int job = blockIdx.x * kSRefs + (threadIdx.x >> 5) * 16 + (lane & 15);
+    const bool live = job < jobs;
+    const int n = live ? count[job] : 0;
+    int32_t* op = pos + (int64_t)(live ? job : 0) * G;
+    int32_t* os = slot + (int64_t)(live ? job : 0) * G;
+    float* od = dist + (int64_t)(live ? job : 0) * G;
+    if (live && half == 0)
+        for (int q = 0; q < G; ++q) os[q] = q < n ? t0 : -1;
+    const bool search = live && n > 0 && ntemp > 1 && first < last;
+    // a warp with no searching reference leaves (uniform: no shuffle is pending)
+    if (!__any_sync(0xffffffffu, search)) return;
+    const int cx = search ? pos_x(op[0]) : 0, cy = search ? pos_y(op[0]) : 0;
+    const int64_t rs = tp.stride[t0];
+    float2 rf[B][2];
+    {
+        const float* refp = tp.plane[t0] + (int64_t)cy * rs + cx + 4 * half;
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            rf[i][0] = make_float2(__ldg(refp + i * rs), __ldg(refp + i * rs + 1));
+            rf[i][1] = make_float2(__ldg(refp + i * rs + 2), __ldg(refp + i * rs + 3));
+        }
+    }
+    // the group so far: the spatial matches without the reference itself
+    LaneTop<K> group;
+    group.init();
+    for (int i = 1; i < (search ? n : 0); ++i)
+        group.add(tk64(canon(od[i]), (uint32_t(t0) << 26) | (uint32_t(pos_y(op[i])) << 13) | uint32_t(pos_x(op[i]))));
+    // window centres per direction: the first ps_num of the spatial group
+    int cxs[2][PS], cys[2][PS], nc[2];
+    const int nseed = search ? min(n, ps_num) : 0;
+#pragma unroll
+    for (int q = 0; q < PS; ++q) {
+        const int32_t p = q < nseed ? op[q] : 0;
+        cxs[0][q] = cxs[1][q] = pos_x(p);
+        cys[0][q] = cys[1][q] = pos_y(p);
+    }
+    nc[0] = nc[1] = nseed;
+    const int maxx = W - B, maxy = H - B;
+    const float2 neg1 = make_float2(-1.f, -1.f);
+    for (int dt = 1; dt <= (ntemp - 1) / 2; ++dt) {
+#pragma unroll
+        for (int dir = 0; dir < 2; ++dir) {
+            const int t = t0 + (dir == 0 ? -dt : dt);
+            if (t < first || t >= last) continue;  // the same for the whole warp
+            const float* pl = tp.plane[t];
+            const int64_t ps = tp.stride[t];
+            LaneTop<PS> layer;
+            layer.init();
+#pragma unroll
+            for (int i = 0; i < PS; ++i) {
+                const bool win = i < nc[dir];
+                const int xa = max(0, cxs[dir][i] - PR), xb = min(maxx, cxs[dir][i] + PR);
+                const int ya = max(0, cys[dir][i] - PR), yb = min(maxy, cys[dir][i] + PR);
+                const int nk = win ? yb - ya + 1 : 0;
+                for (int col = 0; col < SPAN; ++col) {
+                    const int x = xa + col;
+                    const bool colok = win && x <= xb;
+                    const float* colp = pl + (int64_t)(colok ? ya : 0) * ps + (colok ? x : 0) + 4 * half;
+                    float2 acc[8][2];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int srow = 0; srow < ROWS; ++srow) {
+                        float2 p01 = make_float2(0.f, 0.f), p23 = make_float2(0.f, 0.f);
+                        if (colok && srow < nk + B - 1) {
+                            const float* rowp = colp + (int64_t)srow * ps;
+                            p01 = make_float2(__ldg(rowp), __ldg(rowp + 1));
+                            p23 = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
+                        }
+#pragma unroll
+                        for (int ii = 0; ii < B; ++ii) {
+                            const int k = srow - ii;
+                            if (k >= 0 && k < SPAN) {
+                                const float2 d01 = __ffma2_rn(p01, neg1, rf[ii][0]);
+                                const float2 d23 = __ffma2_rn(p23, neg1, rf[ii][1]);
+                                acc[k & 7][0] = __ffma2_rn(d01, d01, acc[k & 7][0]);
+                                acc[k & 7][1] = __ffma2_rn(d23, d23, acc[k & 7][1]);
+                            }
+                        }
+                        const int kd = srow - (B - 1);
+                        if (kd >= 0 && kd < SPAN) {
+                            const float2 a = acc[kd & 7][0], b = acc[kd & 7][1];
+                            acc[kd & 7][0] = acc[kd & 7][1] = make_float2(0.f, 0.f);
+                            const float hs = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
+                            const float dd = __fadd_rn(hs, __shfl_xor_sync(0xffffffffu, hs, 16));
+                            if (colok && kd < nk) {
+                                const int y = ya + kd;
+                                bool dup = false;
+#pragma unroll
+                                for (int j = 0; j < PS; ++j)
+                                    if (j < i)
+                                        dup |= x >= max(0, cxs[dir][j] - PR) && x <= min(maxx, cxs[dir][j] + PR) &&
+                                               y >= max(0, cys[dir][j] - PR) && y <= min(maxy, cys[dir][j] + PR);
+                                if (!dup)
+                                    layer.add(tk64(canon(dd), (uint32_t(t) << 26) | (uint32_t(y) << 13) | uint32_t(x)));
+                            }
+                        }
+                    }
+                }
+            }
+            // the layer's best: into the group, and the next layer's centres
+            int got = 0;
+#pragma unroll
+            for (int q = 0; q < PS; ++q) {
+                const uint64_t k = layer.k[q];
+                if (q < ps_num && k != ~0ull) {
+                    group.add(k);
+                    cxs[dir][q] = int(k & 0x1fff);
+                    cys[dir][q] = int((k >> 13) & 0x1fff);
+                    ++got;
+                }
+            }
+            nc[dir] = got;
+        }
+    }
+    if (!search || half != 0) return;
+    int nb = 0;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const bool valid = group.k[q] != ~0ull;
+        nb += valid;
+        const uint32_t tyx = uint32_t(group.k[q]);
+        op[1 + q] = valid ? pack_pos(tyx & 0x1fff, (tyx >> 13) & 0x1fff) : -1;
+        os[1 + q] = valid ? int32_t(tyx >> 26) : -1;
+        od[1 + q] = valid ? __uint_as_float(uint32_t(group.k[q] >> 32)) : 0.f;
+    }
+    os[0] = t0;
+    count[job] = 1 + nb;
+}
+
 }  // namespace
 
 void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int valid_begin, int valid_end,
@@ -458,6 +611,25 @@ void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int 
                                                  ps_range, jobs, pos, slot, dist, count);
         };
         const bool r4 = ps_range == 4;
+        if (r4 && ps_num <= 2 && (group == 2 || group == 4 || group == 8 || group == 16)) {
+            const dim3 gs(ceil_div(jobs, kSRefs));
+            auto gos = [&](auto kern) {
+                kern<<<gs, 2 * kSRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, ps_num, jobs, pos,
+                                                    slot, dist, count);
+            };
+            switch (group * 4 + ps_num) {
+                case 9: gos(temporal8s_kernel<1, 1, 4>); break;
+                case 10: gos(temporal8s_kernel<1, 2, 4>); break;
+                case 17: gos(temporal8s_kernel<3, 1, 4>); break;
+                case 18: gos(temporal8s_kernel<3, 2, 4>); break;
+                case 33: gos(temporal8s_kernel<7, 1, 4>); break;
+                case 34: gos(temporal8s_kernel<7, 2, 4>); break;
+                case 65: gos(temporal8s_kernel<15, 1, 4>); break;
+                default: gos(temporal8s_kernel<15, 2, 4>); break;
+            }
+            NSSB_CUDA(cudaGetLastError());
+            return;
+        }
         if (ps_num <= 2) r4 ? go(temporal8_kernel<2, 4>) : go(temporal8_kernel<2, 0>);
         else if (ps_num <= 4) r4 ? go(temporal8_kernel<4, 4>) : go(temporal8_kernel<4, 0>);
         else r4 ? go(temporal8_kernel<8, 4>) : go(temporal8_kernel<8, 0>);
