@@ -287,6 +287,40 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
     }
 }
 
+// Temporal centre, batched over its planes: each plane with its own slots.
+template <int G, bool WIENER>
+__global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const __grid_constant__ GroupSlotBatch gb) {
+    using Sh = Shape<G>;
+    constexpr int CUBE = G * Sh::S;
+    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / Sh::LP;
+    const int stride_w = gridDim.x * kWarps;
+    int pl = 0;
+    for (int job = blockIdx.x * kWarps + warp; job < gb.total_jobs; job += stride_w) {
+        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= job) ++pl;
+        const GroupSlotPlane& P_ = gb.p[pl];
+        const GroupIO& io = P_.io;
+        const int lj = job - P_.job0;
+        const int k = P_.count[lj];
+        if (k <= 0) continue;
+        const int32_t p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
+        const int s = (P_.slot && g < k) ? P_.slot[(size_t)lj * G + g] : 0;
+        filter_group<G, WIENER>(
+            smem[warp], smem[warp] + CUBE, lane, k, p, s, P_.sigma,
+            [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
+            [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
+            [&](int sl, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(io.num[sl] + (int64_t)y * io.acc_stride + x),
+                          (unsigned long long)v);
+            },
+            [&](int sl, int x, int y, long long v) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
+                          (unsigned long long)v);
+            });
+    }
+}
+
 // Batched form: every job of every plane of the batch, a warp per group.
 template <int G, bool WIENER, int NW>
 __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_constant__ GroupBatch gb) {
@@ -373,6 +407,23 @@ bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, c
             return true;
         default:
             return false;
+    }
+}
+
+bool launch_group8_slots_batch(const GroupSlotBatch& gb, int group, bool wiener, cudaStream_t stream) {
+    if (gb.total_jobs <= 0) return true;
+    const int blocks = std::min(ceil_div(gb.total_jobs, kWarps), 148 * 16);
+    auto go = [&](auto kern) {
+        kern<<<blocks, 32 * kWarps, 0, stream>>>(gb);
+        NSSB_CUDA(cudaGetLastError());
+    };
+    switch (group) {
+        case 4: wiener ? go(group8_slots_batch_kernel<4, true>) : go(group8_slots_batch_kernel<4, false>); return true;
+        case 8: wiener ? go(group8_slots_batch_kernel<8, true>) : go(group8_slots_batch_kernel<8, false>); return true;
+        case 16:
+            wiener ? go(group8_slots_batch_kernel<16, true>) : go(group8_slots_batch_kernel<16, false>);
+            return true;
+        default: return false;
     }
 }
 

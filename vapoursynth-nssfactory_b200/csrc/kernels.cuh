@@ -114,6 +114,22 @@ struct TemporalPlanes {
 void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int valid_begin, int valid_end,
                            int width, int height, int block, int step, int group, int ps_num, int ps_range,
                            int32_t* pos, int32_t* slot, float* dist, int32_t* count, cudaStream_t stream);
+// The temporal layers of up to three planes of one centre in one launch (the
+// streaming kernel: 8x8 blocks, ps_range 4, ps_num <= 2, groups 2/4/8/16);
+// false when the shape is not covered (launch per plane instead).
+struct TemporalBatchPlane {
+    TemporalPlanes tp;
+    int W, H, jobs, cta0;
+    int32_t* pos;
+    int32_t* slot;
+    float* dist;
+    int32_t* count;
+};
+struct TemporalBatch {
+    int n, ntemp, t0, first, last, group, ps_num, ps_range, total_ctas;
+    TemporalBatchPlane p[3];
+};
+bool launch_match_temporal_batch(TemporalBatch& batch, cudaStream_t stream);
 
 // Group filtering + aggregation of one stage (hard threshold, or Wiener when
 // ref planes are given). Sums go to fixed-point num (per pixel) and wsum (per
@@ -134,6 +150,20 @@ void launch_group_filter(const GroupIO& io, int width, int height, const int32_t
 // (group8.cu); false when the shape has none.
 bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, const int32_t* count, int njobs,
                    int group, float sigma, bool wiener, cudaStream_t stream);
+// The same over up to three planes of one temporal centre in one launch.
+struct GroupSlotPlane {
+    GroupIO io;
+    const int32_t* pos;
+    const int32_t* slot;
+    const int32_t* count;
+    int njobs, job0;
+    float sigma;
+};
+struct GroupSlotBatch {
+    int n, total_jobs;
+    GroupSlotPlane p[3];
+};
+bool launch_group8_slots_batch(const GroupSlotBatch& batch, int group, bool wiener, cudaStream_t stream);
 // Device scratch (floats) the generic group kernel needs for this shape, 0 if none.
 size_t group_filter_scratch_floats(int block, int group, bool wiener);
 

@@ -452,16 +452,23 @@ __global__ void __launch_bounds__(32 * kTRefs, 4)
 // reference keep identical lists: the layer's PS best, and the group itself
 // (spatial matches, then every layer's best, inserted as they are found --
 // the same set, hence the same top, as the reference's merge).
-constexpr int kSRefs = 64;  // references per CTA (4 warps)
+constexpr int kSRefs = 32;  // references per CTA (2 warps)
 
 template <int K, int PS, int PR>
-__global__ void __launch_bounds__(2 * kSRefs, 4)
-    temporal8s_kernel(TemporalPlanes tp, int ntemp, int t0, int first, int last, int W, int H, int ps_num,
-                      int jobs, int32_t* __restrict__ pos, int32_t* __restrict__ slot, float* __restrict__ dist,
-                      int32_t* __restrict__ count) {
+__global__ void __launch_bounds__(2 * kSRefs, 8) temporal8s_kernel(const __grid_constant__ TemporalBatch tb) {
     constexpr int B = 8, G = K + 1, SPAN = 2 * PR + 1, ROWS = SPAN + B - 1;
+    int pl = 0;
+    while (pl + 1 < tb.n && tb.p[pl + 1].cta0 <= (int)blockIdx.x) ++pl;
+    const TemporalBatchPlane& P = tb.p[pl];
+    const TemporalPlanes& tp = P.tp;
+    const int ntemp = tb.ntemp, t0 = tb.t0, first = tb.first, last = tb.last, ps_num = tb.ps_num;
+    const int W = P.W, H = P.H, jobs = P.jobs;
+    int32_t* __restrict__ pos = P.pos;
+    int32_t* __restrict__ slot = P.slot;
+    float* __restrict__ dist = P.dist;
+    int32_t* __restrict__ count = P.count;
     const int lane = threadIdx.x & 31, half = lane >> 4;
-    const int job = blockIdx.x * kSRefs + (threadIdx.x >> 5) * 16 + (lane & 15);
+    const int job = (blockIdx.x - P.cta0) * kSRefs + (threadIdx.x >> 5) * 16 + (lane & 15);
     const bool live = job < jobs;
     const int n = live ? count[job] : 0;
     int32_t* op = pos + (int64_t)(live ? job : 0) * G;
@@ -593,6 +600,39 @@ __global__ void __launch_bounds__(2 * kSRefs, 4)
 
 }  // namespace
 
+bool launch_match_temporal_batch(TemporalBatch& tb, cudaStream_t stream) {
+    const int g = tb.group;
+    if (tb.n < 1 || tb.n > 3 || tb.ps_range != 4 || tb.ps_num < 1 || tb.ps_num > 2 || tb.ntemp > 33 ||
+        !(g == 2 || g == 4 || g == 8 || g == 16))
+        return false;
+    int ctas = 0;
+    for (int i = 0; i < tb.n; ++i) {
+        TemporalBatchPlane& p = tb.p[i];
+        if (p.W >= 8192 || p.H >= 8192 || p.W < 8 || p.H < 8) return false;
+        p.cta0 = ctas;
+        ctas += ceil_div(p.jobs, kSRefs);
+    }
+    tb.total_ctas = ctas;
+    if (ctas == 0) return true;
+    const int first = tb.first < 0 ? 0 : tb.first;
+    const int last = tb.last < 0 ? tb.ntemp : (tb.last < tb.ntemp ? tb.last : tb.ntemp);
+    tb.first = first;
+    tb.last = last;
+    auto gos = [&](auto kern) { kern<<<ctas, 2 * kSRefs, 0, stream>>>(tb); };
+    switch (g * 4 + tb.ps_num) {
+        case 9: gos(temporal8s_kernel<1, 1, 4>); break;
+        case 10: gos(temporal8s_kernel<1, 2, 4>); break;
+        case 17: gos(temporal8s_kernel<3, 1, 4>); break;
+        case 18: gos(temporal8s_kernel<3, 2, 4>); break;
+        case 33: gos(temporal8s_kernel<7, 1, 4>); break;
+        case 34: gos(temporal8s_kernel<7, 2, 4>); break;
+        case 65: gos(temporal8s_kernel<15, 1, 4>); break;
+        default: gos(temporal8s_kernel<15, 2, 4>); break;
+    }
+    NSSB_CUDA(cudaGetLastError());
+    return true;
+}
+
 void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int valid_begin, int valid_end,
                            int width, int height, int block, int step, int group, int ps_num, int ps_range,
                            int32_t* pos, int32_t* slot, float* dist, int32_t* count, cudaStream_t stream) {
@@ -612,23 +652,17 @@ void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int 
         };
         const bool r4 = ps_range == 4;
         if (r4 && ps_num <= 2 && (group == 2 || group == 4 || group == 8 || group == 16)) {
-            const dim3 gs(ceil_div(jobs, kSRefs));
-            auto gos = [&](auto kern) {
-                kern<<<gs, 2 * kSRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, ps_num, jobs, pos,
-                                                    slot, dist, count);
-            };
-            switch (group * 4 + ps_num) {
-                case 9: gos(temporal8s_kernel<1, 1, 4>); break;
-                case 10: gos(temporal8s_kernel<1, 2, 4>); break;
-                case 17: gos(temporal8s_kernel<3, 1, 4>); break;
-                case 18: gos(temporal8s_kernel<3, 2, 4>); break;
-                case 33: gos(temporal8s_kernel<7, 1, 4>); break;
-                case 34: gos(temporal8s_kernel<7, 2, 4>); break;
-                case 65: gos(temporal8s_kernel<15, 1, 4>); break;
-                default: gos(temporal8s_kernel<15, 2, 4>); break;
-            }
-            NSSB_CUDA(cudaGetLastError());
-            return;
+            static thread_local TemporalBatch tb;
+            tb.n = 1;
+            tb.ntemp = ntemp;
+            tb.t0 = t0;
+            tb.first = first;
+            tb.last = last;
+            tb.group = group;
+            tb.ps_num = ps_num;
+            tb.ps_range = ps_range;
+            tb.p[0] = TemporalBatchPlane{planes, width, height, jobs, 0, pos, slot, dist, count};
+            if (launch_match_temporal_batch(tb, stream)) return;
         }
         if (ps_num <= 2) r4 ? go(temporal8_kernel<2, 4>) : go(temporal8_kernel<2, 0>);
         else if (ps_num <= 4) r4 ? go(temporal8_kernel<4, 4>) : go(temporal8_kernel<4, 0>);

@@ -205,39 +205,95 @@ private:
             src(f, sp[t], ss[t]);
             if (wiener_) ref(f, rp[t], rs[t]);
         }
-        bool matched0 = false;
+        // the planes that match: every plane with a sigma, or plane 0 alone for
+        // CBM3D (its groups serve every plane, filter_bm3d.cpp:451-486)
+        int mpl[3], nm = 0;
+        bool any = false;
+        for (int p = 0; p < cfg_.planes; ++p) any |= sp_[p].sigma != 0.f;
+        if (cfg_.chroma) {
+            if (any) mpl[nm++] = 0;
+        } else {
+            for (int p = 0; p < cfg_.planes; ++p)
+                if (sp_[p].sigma != 0.f) mpl[nm++] = p;
+        }
+        auto same_match = [&](const StageParams& a, const StageParams& b) {
+            return a.block == b.block && a.step == b.step && a.bm_range == b.bm_range && a.group == b.group &&
+                   a.ps_num == b.ps_num && a.ps_range == b.ps_range;
+        };
+        bool uniform = nm > 0;
+        for (int q = 1; q < nm; ++q) uniform &= same_match(sp_[mpl[q]], sp_[mpl[0]]);
+        TemporalPlanes tps[3]{};
+        for (int q = 0; q < nm; ++q)
+            for (int t = 0; t < ntemp; ++t) {
+                tps[q].plane[t] = wiener_ ? rp[t][mpl[q]] : sp[t][mpl[q]];
+                tps[q].stride[t] = wiener_ ? rs[t][mpl[q]] : ss[t][mpl[q]];
+            }
+        if (nm > 0) {
+            clock_->begin(StageClock::kMatch);
+            for (int q = 0; q < nm; ++q) clock_->count_match(cfg_.plane_w[mpl[q]], cfg_.plane_h[mpl[q]], sp_[mpl[q]]);
+            // the centre frame: one batched launch over the planes when they share a shape
+            bool done = false;
+            const StageParams& m0 = sp_[mpl[0]];
+            if (uniform && m0.block == 8) {
+                mbatch_.n = nm;
+                mbatch_.step = m0.step;
+                for (int q = 0; q < nm; ++q) {
+                    const int mp = mpl[q];
+                    mbatch_.p[q] = MatchPlane{tps[q].plane[r_], tps[q].stride[r_], pos_[mp], dist_[mp], count_[mp],
+                                              cfg_.plane_w[mp], cfg_.plane_h[mp], 0, 0, 0};
+                }
+                if (tune_ && tune_->form == 1 && tune_->tc)
+                    done = launch_match_tc_batch(mbatch_, m0.bm_range, m0.group, tune_->tc, stream_);
+                if (!done) done = launch_match8_batch(mbatch_, m0.bm_range, m0.group, stream_);
+            }
+            if (!done)
+                for (int q = 0; q < nm; ++q) {
+                    const int mp = mpl[q];
+                    const StageParams& ms = sp_[mp];
+                    launch_match_spatial(tps[q].plane[r_], tps[q].stride[r_], cfg_.plane_w[mp], cfg_.plane_h[mp],
+                                         ms.block, ms.step, ms.bm_range, ms.group, pos_[mp], dist_[mp], count_[mp],
+                                         stream_);
+                }
+            // the temporal layers: one launch over the planes when the streaming kernel covers them
+            done = false;
+            if (uniform && m0.block == 8) {
+                tbatch_.n = nm;
+                tbatch_.ntemp = ntemp;
+                tbatch_.t0 = r_;
+                tbatch_.first = vbegin;
+                tbatch_.last = vend;
+                tbatch_.group = m0.group;
+                tbatch_.ps_num = m0.ps_num;
+                tbatch_.ps_range = m0.ps_range;
+                for (int q = 0; q < nm; ++q) {
+                    const int mp = mpl[q];
+                    const int jobs = grid_count(cfg_.plane_w[mp], m0.block, m0.step) *
+                                     grid_count(cfg_.plane_h[mp], m0.block, m0.step);
+                    tbatch_.p[q] = TemporalBatchPlane{tps[q], cfg_.plane_w[mp], cfg_.plane_h[mp], jobs, 0,
+                                                      pos_[mp], slot_[mp], dist_[mp], count_[mp]};
+                }
+                done = launch_match_temporal_batch(tbatch_, stream_);
+            }
+            if (!done)
+                for (int q = 0; q < nm; ++q) {
+                    const int mp = mpl[q];
+                    const StageParams& ms = sp_[mp];
+                    launch_match_temporal(tps[q], ntemp, r_, vbegin, vend, cfg_.plane_w[mp], cfg_.plane_h[mp],
+                                          ms.block, ms.step, ms.group, ms.ps_num, ms.ps_range, pos_[mp], slot_[mp],
+                                          dist_[mp], count_[mp], stream_);
+                }
+            clock_->end(StageClock::kMatch);
+        }
+        // group filtering into the target frames' sums
+        gbatch_.n = 0;
+        gbatch_.total_jobs = 0;
+        bool batchable = true;
+        int gshape = -1;
         for (int p = 0; p < cfg_.planes; ++p) {
             const StageParams& st = sp_[p];
             if (st.sigma == 0.f) continue;
             const int w = cfg_.plane_w[p], h = cfg_.plane_h[p];
-            // CBM3D: the groups of plane 0 serve every plane (matched once per centre)
             const int mp = cfg_.chroma ? 0 : p;
-            if (!cfg_.chroma || !matched0) {
-                TemporalPlanes tp{};
-                for (int t = 0; t < ntemp; ++t) {
-                    tp.plane[t] = wiener_ ? rp[t][mp] : sp[t][mp];
-                    tp.stride[t] = wiener_ ? rs[t][mp] : ss[t][mp];
-                }
-                const StageParams& ms = sp_[mp];
-                clock_->count_match(cfg_.plane_w[mp], cfg_.plane_h[mp], ms);
-                clock_->begin(StageClock::kMatch);
-                bool tc = false;
-                if (tune_ && tune_->form == 1 && tune_->tc && ms.block == 8) {
-                    mbatch_.n = 1;
-                    mbatch_.step = ms.step;
-                    mbatch_.p[0] = MatchPlane{tp.plane[r_], tp.stride[r_], pos_[mp], dist_[mp], count_[mp],
-                                              cfg_.plane_w[mp], cfg_.plane_h[mp], 0, 0, 0};
-                    tc = launch_match_tc_batch(mbatch_, ms.bm_range, ms.group, tune_->tc, stream_);
-                }
-                if (!tc)
-                    launch_match_spatial(tp.plane[r_], tp.stride[r_], cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
-                                         ms.step, ms.bm_range, ms.group, pos_[mp], dist_[mp], count_[mp], stream_);
-                launch_match_temporal(tp, ntemp, r_, vbegin, vend, cfg_.plane_w[mp], cfg_.plane_h[mp], ms.block,
-                                      ms.step, ms.group, ms.ps_num, ms.ps_range, pos_[mp], slot_[mp], dist_[mp],
-                                      count_[mp], stream_);
-                clock_->end(StageClock::kMatch);
-                matched0 = true;
-            }
             GroupIO io{};
             const int64_t stride = ss[r_][p], rstride = wiener_ ? rs[r_][p] : 0;
             for (int t = 0; t < ntemp; ++t) {
@@ -254,9 +310,24 @@ private:
             io.ref_stride = rstride;
             io.acc_stride = pitch_[p];
             const int jobs = grid_count(w, st.block, st.step) * grid_count(h, st.block, st.step);
+            const bool fits = st.block == 8 && (st.group == 4 || st.group == 8 || st.group == 16) &&
+                              (gshape < 0 || gshape == st.group);
+            if (batchable && fits) {
+                gshape = st.group;
+                gbatch_.p[gbatch_.n++] = GroupSlotPlane{io, pos_[mp], slot_[mp], count_[mp], jobs,
+                                                         gbatch_.total_jobs, st.sigma};
+                gbatch_.total_jobs += jobs;
+            } else {
+                batchable = false;
+                clock_->begin(StageClock::kGroup);
+                launch_group_filter(io, w, h, pos_[mp], slot_[mp], count_[mp], jobs, st.block, st.group, st.sigma,
+                                    wiener_, cube_[p], cube_floats_[p], stream_);
+                clock_->end(StageClock::kGroup);
+            }
+        }
+        if (gbatch_.n > 0) {
             clock_->begin(StageClock::kGroup);
-            launch_group_filter(io, w, h, pos_[mp], slot_[mp], count_[mp], jobs, st.block, st.group, st.sigma,
-                                wiener_, cube_[p], cube_floats_[p], stream_);
+            launch_group8_slots_batch(gbatch_, gshape, wiener_, stream_);
             clock_->end(StageClock::kGroup);
         }
         if (!legacy) {
@@ -289,6 +360,8 @@ private:
     const MatchTune* tune_;  // the engine's matcher form (read at each centre)
     StageClock* clock_;      // the engine's launch accounting
     MatchBatch mbatch_;
+    TemporalBatch tbatch_;
+    GroupSlotBatch gbatch_;
 };
 
 // Device frames of the temporal window: host frames are uploaded once and kept
