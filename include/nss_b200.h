@@ -111,6 +111,20 @@ typedef struct nssb_frame_out {
 int nssb_bm3d_get_frame(nssb_bm3d* h, int n, const nssb_frame* clip_frames, const nssb_frame* ref_frames, int first,
                         int count, int memory, nssb_frame_out* out);
 
+/* Frame properties the filter stamps on output frame n (stamp_contribution,
+ * src/frontend/contribution.hpp:12-27; constants include/nss/contracts.hpp:6-17
+ * of the reference): _NSSModel = 1 (BM3D), _NSSModelVersion = 3,
+ * _NSSNoiseProfile = 1, and on the legacy temporal intermediate also
+ * _NSSFatVersion = 2, _NSSFatRadius = r, _NSSFatCenter = n, _NSSFatLayout = 1
+ * (num/den slices), which nss.VAggregate checks. A shim copies the source
+ * frame's properties, then sets these (and deletes the _NSSFat* keys when
+ * they are not listed). Writes up to cap entries and their number to *count. */
+typedef struct nssb_prop {
+    const char* key; /* static string */
+    int64_t value;
+} nssb_prop;
+int nssb_bm3d_frame_props(const nssb_bm3d* h, int n, nssb_prop* out, int cap, int* count);
+
 /* Kernel accounting of a handle, for measurement (no reference counterpart;
  * the reference measures through Nsight, tests/cuda/run_ncu.py). With
  * timing on, the engine brackets its matching, group and finish launches

@@ -136,3 +136,13 @@ def test_temporal_yuv420_device_frames(nssb, oracle, synth, dev):
     for p in range(3):
         want = oracle.bm3d_clip_plane([f[p] for f in frames], sts[p], radius)
         assert oracle.psnr([h[p] for h in host], want) >= MIN_PSNR
+
+
+def test_frame_props(nssb, synth, dev):
+    frames = gray_clip(synth, 3, 64, 48, 10)
+    clip = nssb.Clip.from_frames([(f,) for f in frames], nssb.GRAY)
+    base = {"_NSSModel": 1, "_NSSModelVersion": 3, "_NSSNoiseProfile": 1}
+    assert nssb.BM3D(clip, sigma=10).frame_props(1) == base
+    assert nssb.BM3D(clip, sigma=10, radius=1).frame_props(2) == base  # rolling: finished frames
+    fat = nssb.BM3D(clip, sigma=10, radius=1, temporal_mode="legacy").frame_props(2)
+    assert fat == {**base, "_NSSFatVersion": 2, "_NSSFatRadius": 1, "_NSSFatCenter": 2, "_NSSFatLayout": 1}

@@ -94,6 +94,10 @@ class KernelStats(C.Structure):
 _lib = None
 
 
+class Prop(C.Structure):
+    _fields_ = [("key", C.c_char_p), ("value", C.c_int64)]
+
+
 class TcStats(C.Structure):
     _fields_ = [("survivors", C.c_int64), ("refs", C.c_int64), ("max_error_ratio", C.c_float),
                 ("flagged_tiles", C.c_int), ("timeouts", C.c_int)]
@@ -168,6 +172,7 @@ def lib():
         L.nssb_bm3d_plane_stage_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                                     C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.nssb_bm3d_set_matcher.argtypes = [C.c_void_p, C.c_int]
+        L.nssb_bm3d_frame_props.argtypes = [C.c_void_p, C.c_int, C.POINTER(Prop), C.c_int, C.POINTER(C.c_int)]
         L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
         L.nssb_batch_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
@@ -309,6 +314,13 @@ class Node:
         st = KernelStats()
         check(lib().nssb_bm3d_stats(self.handle, int(enable_timing), int(reset), C.byref(st)))
         return st
+
+    def frame_props(self, n: int) -> dict:
+        """The properties stamped on output frame n (_NSSModel, ..., _NSSFat* on the legacy intermediate)."""
+        arr = (Prop * 8)()
+        k = C.c_int()
+        check(lib().nssb_bm3d_frame_props(self.handle, n, arr, 8, C.byref(k)))
+        return {arr[i].key.decode(): arr[i].value for i in range(k.value)}
 
     def set_matcher(self, form: int) -> None:
         """0: FP32 matcher (default); 1: tensor-core precision form (identical lists)."""

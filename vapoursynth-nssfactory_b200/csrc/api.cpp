@@ -185,6 +185,25 @@ int nssb_match_spatial(const float* plane, int64_t stride, int width, int height
     });
 }
 
+int nssb_bm3d_frame_props(const nssb_bm3d* h, int n, nssb_prop* out, int cap, int* count) {
+    if (count) *count = 0;
+    return guarded([&] {
+        if (!h || !count || cap < 0 || (cap > 0 && !out)) throw std::invalid_argument("nssb_bm3d_frame_props: invalid arguments");
+        const nssb::Bm3dConfig& c = h->engine->config();
+        if (n < 0 || n >= c.vi.num_frames) throw std::out_of_range("nss_cuda.BM3D: frame number out of range");
+        nssb_prop props[7] = {{"_NSSModel", 1}, {"_NSSModelVersion", 3}, {"_NSSNoiseProfile", 1}};
+        int k = 3;
+        if (c.radius > 0 && !c.rolling) {  // the fat intermediate: one centre's num/den slices
+            props[k++] = {"_NSSFatVersion", 2};
+            props[k++] = {"_NSSFatRadius", c.radius};
+            props[k++] = {"_NSSFatCenter", n};
+            props[k++] = {"_NSSFatLayout", 1};
+        }
+        for (int i = 0; i < k && i < cap; ++i) out[i] = props[i];
+        *count = k < cap ? k : cap;
+    });
+}
+
 int nssb_bm3d_set_matcher(nssb_bm3d* h, int form) {
     return guarded([&] {
         if (!h) throw std::invalid_argument("nssb_bm3d_set_matcher: invalid handle");

@@ -1,4 +1,5 @@
-// Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape.
+// Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape
+// (bm_range 9), and the ranges 4-9, 12 and 15.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
 // keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
@@ -273,10 +274,14 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
 
 template <int R, int K>
 void launch_rk(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
-    switch (tune.parts) {
-        case 1: launch_rkp<R, K, 1>(mb, tune, stream); break;
-        case 4: launch_rkp<R, K, 4>(mb, tune, stream); break;
-        default: launch_rkp<R, K, 2>(mb, tune, stream); break;
+    if constexpr (R == 9) {  // the default range: every column split the tuner may pick
+        switch (tune.parts) {
+            case 1: launch_rkp<R, K, 1>(mb, tune, stream); break;
+            case 4: launch_rkp<R, K, 4>(mb, tune, stream); break;
+            default: launch_rkp<R, K, 2>(mb, tune, stream); break;
+        }
+    } else {
+        launch_rkp<R, K, 2>(mb, tune, stream);
     }
 }
 
@@ -298,8 +303,16 @@ bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t s
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8) return false;
     const MatchTune t = tune ? *tune : MatchTune{};
+    // ranges up to 15: a column's 2R + 1 candidates fit the 32-bit pass mask
     switch (bm_range) {
+        case 4: return launch_r<4>(mb, group, t, stream);
+        case 5: return launch_r<5>(mb, group, t, stream);
+        case 6: return launch_r<6>(mb, group, t, stream);
+        case 7: return launch_r<7>(mb, group, t, stream);
+        case 8: return launch_r<8>(mb, group, t, stream);
         case 9: return launch_r<9>(mb, group, t, stream);
+        case 12: return launch_r<12>(mb, group, t, stream);
+        case 15: return launch_r<15>(mb, group, t, stream);
         default: return false;
     }
 }
