@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--served", type=int, default=2000, help="requests of the serving leg (0: skip it)")
     ap.add_argument("--no-legs", action="store_true", help="skip the temporal (C3) and mixed-batch (C4) legs")
+    ap.add_argument("--served-workers", type=int, default=8, help="temporal requests the server runs at once")
     ap.add_argument("--c3-frames", type=int, default=60)
     ap.add_argument("--served-plain", type=int, default=300,
                     help="requests of the same stream rendered by the per-frame drop-in for comparison")
@@ -341,7 +342,9 @@ def our_arm(args):
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
         out["batched_c4"] = c4_leg(nssb, synth, dev)
     if args.served > 0:
-        out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain))
+        out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
+                                   args.served_workers)
+        out["served"]["workers"] = args.served_workers
         out["served"]["note"] = ("seeded Poisson arrivals at 200 req/s; latency = submission -> outputs in pinned "
                                  "host memory; per rank")
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -539,7 +542,7 @@ def served_workload(n_req, rate=200.0, seed=2024):
             for i in range(n_req)]
 
 
-def served_leg(nssb, synth, local, n_req, n_plain):
+def served_leg(nssb, synth, local, n_req, n_plain, workers=8):
     """The serving form on the request stream above, then the per-frame drop-in
     (a BM3D node per request, first come first served) on its first n_plain
     requests with the same arrival times. Latency: arrival -> all outputs in
@@ -558,7 +561,7 @@ def served_leg(nssb, synth, local, n_req, n_plain):
                       for f in frames]
         for k in range(1, 9):
             clips[(name, k)] = nssb.Clip.from_frames(pool[name][:k], nssb.YUV, 1, 1)
-    srv = nssb.Server(device_id=local)
+    srv = nssb.Server(device_id=local, workers=workers)
     # warm-up: every (resolution, radius) once, so engines and kernels are loaded
     for name in SERVED_RES:
         for r in range(3):
