@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-legs", action="store_true", help="skip the temporal (C3) and mixed-batch (C4) legs")
     ap.add_argument("--served-workers", type=int, default=8, help="temporal requests the server runs at once")
     ap.add_argument("--c3-frames", type=int, default=60)
+    ap.add_argument("--only", choices=["c3", "c4", "served"], help="run one leg alone (profiling)")
     ap.add_argument("--served-plain", type=int, default=300,
                     help="requests of the same stream rendered by the per-frame drop-in for comparison")
     return ap.parse_args()
@@ -219,6 +220,14 @@ def our_arm(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
+    if args.only:
+        # one leg alone (profiling runs): its JSON object on one line
+        legs = {"c3": lambda: c3_leg(nssb, synth, dev, args.c3_frames, False),
+                "c4": lambda: c4_leg(nssb, synth, dev),
+                "served": lambda: served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
+                                             args.served_workers)}
+        print(json.dumps({"leg": args.only, **legs[args.only]()}), flush=True)
+        return
     nf = args.frames
     frames = synth.yuv420_clip(1000 + rank, W, H, nf, SIGMA)
     dframes = [tuple(torch.from_numpy(p).to(dev) for p in f) for f in frames]

@@ -215,3 +215,17 @@ def test_memory_limit_fits_or_fails_at_creation(nssb, dev):
     b = nssb.BM3D(clip, sigma=10, final=1, memory_limit_mb=4096)
     for n in range(3):
         assert np.array_equal(a.get_frame(n)[0], b.get_frame(n)[0])
+
+
+def test_c1_config_512_gray_hard_threshold(nssb, oracle, dev):
+    """The CPU-runnable benchmark case: one Gray 512x512 frame, sigma 10, final=0, radius 0, defaults."""
+    import importlib
+
+    synth = importlib.import_module("vapoursynth-nssfactory_b200.synth")
+    noisy, clean = synth.gray_frame(2024, 512, 512, 10)
+    node = nssb.BM3D(nssb.Clip.from_frames([(noisy,)], nssb.GRAY), sigma=10)
+    got = node.get_frame(0)[0]
+    st = oracle.stage(oracle.effective_sigma(10.0))
+    want = oracle.bm3d_plane(noisy, st)
+    assert oracle.psnr(got, want) >= 60.0
+    assert oracle.psnr(got, clean) > oracle.psnr(noisy, clean)  # it denoises

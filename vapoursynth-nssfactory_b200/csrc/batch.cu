@@ -406,8 +406,10 @@ BatchPlan& BatchEngine::plan_for(const std::string& sig, int lane) {
     return *plans_.back().second;
 }
 
+constexpr int kMaxChunks = 6, kMinChunkFrames = 4;
+
 // Chunks of the batch: one when every item is on the device (nothing to
-// overlap), else up to four equal chunks so that the host copies of one
+// overlap), else up to six equal chunks so that the host copies of one
 // chunk overlap the kernels of its neighbours.
 std::vector<std::pair<int, int>> BatchEngine::chunks(const BatchItem* items, int n) const {
     bool host = false;
@@ -416,10 +418,13 @@ std::vector<std::pair<int, int>> BatchEngine::chunks(const BatchItem* items, int
     if (opt_.chunk_frames > 0) {
         size = opt_.chunk_frames;
     } else if (host && n >= 2) {
+        // up to kMaxChunks equal chunks of at least kMinChunkFrames frames: the
+        // first upload and the last download are the only copies not hidden
         int k = 0;
-        for (int c = std::min(4, n); c >= 2 && !k; --c)
+        const int most = std::max(1, std::min(kMaxChunks, n / kMinChunkFrames));
+        for (int c = most; c >= 2 && !k; --c)
             if (n % c == 0) k = c;
-        if (!k) k = std::min(4, n);
+        if (!k) k = std::min(most, n);
         size = (n + k - 1) / k;
     }
     std::vector<std::pair<int, int>> out;

@@ -101,7 +101,7 @@ private:
 struct BatchOptions {
     bool autotune = true;
     bool graphs = true;
-    int chunk_frames = 0;  // 0: one chunk for device items, up to 4 equal chunks with host items
+    int chunk_frames = 0;  // 0: one chunk for device items, up to 6 equal chunks with host items
     bool plan_per_stream = false;  // one plan per stream, re-laid out as layouts change (serving)
     LaunchTunes fixed;     // the launch shapes used when autotune is off
 };
