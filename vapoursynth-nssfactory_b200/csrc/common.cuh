@@ -54,4 +54,13 @@ __device__ __forceinline__ float column_tree(const float* c) {
     }
 }
 
+// Asynchronous 4-byte global -> shared copy (LDGSTS): a tile fill issues
+// all its copies without waiting on any, then waits once. bytes = 0 writes
+// zero and reads nothing (src must still be a valid address).
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, int bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 }  // namespace nssb

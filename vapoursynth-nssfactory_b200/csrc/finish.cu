@@ -74,20 +74,27 @@ __global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restri
     dden[(int64_t)y * ds + x] = (float)((double)den[r][c] * kFixedInv);
 }
 
-// Batched finish over a plane table. A CTA finishes a 64 x 32 tile, 8
-// pixels per thread (one column, 8 rows): the origin weights of the tile and
-// its (B-1)-pixel halo, num and src are all requested before the first
-// barrier; den comes from sliding B-wide row sums, then B-tall column sums,
-// exact in int64. num is cleared as it is consumed (each pixel's num is read
-// by exactly one thread), so the next stage finds it zero.
+// Batched finish over a plane table. A CTA finishes a 64 x 32 tile:
+//   - first every thread requests the num and src of its 8 output pixels (8
+//     consecutive pixels of one row), so they arrive while den is formed;
+//   - vertical B-tall sums of the origin weights: a thread per (8-row
+//     quarter, column) of the tile and of its B-1 halo columns on the left
+//     reads 8 + B - 1 weights down its column and slides the sum, exact in
+//     int64, into a shared table vs[32 rows][64 + B - 1 columns];
+//   - horizontal B-wide sums: each thread slides along its 8 pixels.
+// vs column cc is stored at cc + cc / 8 in a row of kVsPitch(B) words with
+// the pitch = 8 (mod 16), so the 16 lanes of a half-warp (2 rows x 8
+// segments) read 16 different bank pairs. num is cleared as it is consumed
+// (each pixel's num is read by exactly one thread), so the next stage finds
+// it zero.
 constexpr int kFX = 64, kFY = 32, kFT = 256;
 
-// BT > 0: the block size known at compile time (8, the default), so the
-// halo tile's loads are a fixed, fully unrolled set issued before any of them
-// is stored; BT = 0: any block size.
+__host__ __device__ constexpr int vs_col(int cc) { return cc + (cc >> 3); }
+__host__ __device__ constexpr int vs_pitch(int B) { return (vs_col(kFX + B - 2) + 1 + 7) / 16 * 16 + 8; }
+
 template <int BT>
 __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant__ FinishBatch fb) {
-    extern __shared__ long long fsm[];  // wt[(kFY + B - 1)][(kFX + B - 1)], then hs[(kFY + B - 1)][kFX]
+    extern __shared__ long long vs[];
     int pl = 0;
     {
         int lo = 0, hi = fb.n - 1;
@@ -99,86 +106,85 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
     }
     const FinishPlane& P = fb.p[pl];
     const int B = BT > 0 ? BT : fb.block;
+    const int pitch = vs_pitch(B);
     const int local = blockIdx.x - P.cta0;
     const int ty = local / P.tiles_x, tx = local - ty * P.tiles_x;
     const int x0 = tx * kFX, y0 = ty * kFY;
-    const int c = threadIdx.x & (kFX - 1), q = threadIdx.x / kFX;  // column, 8-row quarter
-    const int x = x0 + c;
-    // this thread's num and src, requested first
+    // output mapping: row r of the tile, pixels 8 * seg .. 8 * seg + 7
+    const int r = threadIdx.x >> 3, seg = threadIdx.x & 7;
+    const int y = y0 + r, xs = x0 + 8 * seg;
     long long nv[8];
     float sv[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int y = y0 + q * 8 + r;
-        const bool ok = x < P.W && y < P.H;
-        nv[r] = ok ? P.num[(int64_t)y * P.acc_stride + x] : 0;
-        sv[r] = ok ? P.src[(int64_t)y * P.sstride + x] : 0.f;
+    for (int j = 0; j < 8; ++j) {
+        const bool ok = xs + j < P.W && y < P.H;
+        nv[j] = ok ? P.num[(int64_t)y * P.acc_stride + xs + j] : 0;
+        sv[j] = ok ? __ldg(P.src + (int64_t)y * P.sstride + xs + j) : 0.f;
     }
-    const int rows = kFY + B - 1, cols = kFX + B - 1;
-    long long* wtp = fsm;
-    long long* hsp = fsm + rows * cols;
-#define wt(r, cc) wtp[(r) * cols + (cc)]
-#define hs(r, cc) hsp[(r) * kFX + (cc)]
-    if constexpr (BT > 0) {
-        constexpr int kRows = kFY + BT - 1, kCols = kFX + BT - 1, kN = (kRows * kCols + kFT - 1) / kFT;
-        long long v[kN];
+    // vertical sums: quarter q, tile column c (vs column c + B - 1) and, for
+    // c < B - 1, halo column c (vs column c)
+    {
+        const int c = threadIdx.x & (kFX - 1), q = threadIdx.x / kFX;
+        const int ytop = y0 + 8 * q - (B - 1);
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1 && c >= B - 1) break;
+            const int cc = pass == 0 ? c + B - 1 : c;
+            const int xx = x0 - (B - 1) + cc;
+            const bool xok = xx >= 0 && xx < P.W;
+            const long long* col = P.wsum + xx;
+            long long* out = vs + (8 * q) * pitch + vs_col(cc);
+            if constexpr (BT > 0) {
+                long long w[8 + BT - 1];
 #pragma unroll
-        for (int t = 0; t < kN; ++t) {
-            const int i = threadIdx.x + t * kFT;
-            const int r = i / kCols, cc = i - r * kCols;
-            const int yy = y0 - BT + 1 + r, xx = x0 - BT + 1 + cc;
-            v[t] = (i < kRows * kCols && yy >= 0 && yy < P.H && xx >= 0 && xx < P.W)
-                       ? P.wsum[(int64_t)yy * P.acc_stride + xx]
-                       : 0ll;
-        }
+                for (int i = 0; i < 8 + BT - 1; ++i) {
+                    const int yy = ytop + i;
+                    w[i] = (xok && yy >= 0 && yy < P.H) ? __ldg(col + (int64_t)yy * P.acc_stride) : 0ll;
+                }
+                long long sum = 0;
 #pragma unroll
-        for (int t = 0; t < kN; ++t) {
-            const int i = threadIdx.x + t * kFT;
-            if (i < kRows * kCols) wtp[i] = v[t];
-        }
-    } else {
-        for (int i = threadIdx.x; i < rows * cols; i += kFT) {
-            const int r = i / cols, cc = i - r * cols;
-            const int yy = y0 - B + 1 + r, xx = x0 - B + 1 + cc;
-            wt(r, cc) = (yy >= 0 && yy < P.H && xx >= 0 && xx < P.W) ? P.wsum[(int64_t)yy * P.acc_stride + xx] : 0ll;
+                for (int k = 0; k < BT; ++k) sum += w[k];
+                out[0] = sum;
+#pragma unroll
+                for (int rr = 1; rr < 8; ++rr) {
+                    sum += w[rr + BT - 1] - w[rr - 1];
+                    out[rr * pitch] = sum;
+                }
+            } else {
+                const auto at = [&](int i) {
+                    const int yy = ytop + i;
+                    return (xok && yy >= 0 && yy < P.H) ? __ldg(col + (int64_t)yy * P.acc_stride) : 0ll;
+                };
+                long long sum = 0;
+                for (int k = 0; k < B; ++k) sum += at(k);
+                out[0] = sum;
+                for (int rr = 1; rr < 8; ++rr) {
+                    sum += at(rr + B - 1) - at(rr - 1);
+                    out[rr * pitch] = sum;
+                }
+            }
         }
     }
     __syncthreads();
-    // row sums: 8 consecutive columns of one row per task, sliding
-    for (int t = threadIdx.x; t < rows * (kFX / 8); t += kFT) {
-        const int r = t / (kFX / 8), c0 = (t - r * (kFX / 8)) * 8;
-        long long sum = 0;
-        for (int k = 0; k < B; ++k) sum += wt(r, c0 + k);
-        hs(r, c0) = sum;
-#pragma unroll
-        for (int j = 1; j < 8; ++j) {
-            sum += wt(r, c0 + j + B - 1) - wt(r, c0 + j - 1);
-            hs(r, c0 + j) = sum;
-        }
-    }
-    __syncthreads();
-    // column sums down this thread's 8 rows, then the finish
+    // horizontal sums along this thread's 8 pixels, then the finish
+    const long long* row = vs + r * pitch;
     long long den = 0;
-    for (int k = 0; k < B; ++k) den += hs(q * 8 + k, c);
+    for (int k = 0; k < B; ++k) den += row[vs_col(8 * seg + k)];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        if (r > 0) den += hs(q * 8 + r + B - 1, c) - hs(q * 8 + r - 1, c);
-        const int y = y0 + q * 8 + r;
-        if (x < P.W && y < P.H) {
-            P.num[(int64_t)y * P.acc_stride + x] = 0;
+    for (int j = 0; j < 8; ++j) {
+        if (j > 0) den += row[vs_col(8 * seg + j + B - 1)] - row[vs_col(8 * seg + j - 1)];
+        if (xs + j < P.W && y < P.H) {
+            P.num[(int64_t)y * P.acc_stride + xs + j] = 0;
             const float dd = (float)((double)den * kFixedInv);
-            P.dst[(int64_t)y * P.dstride + x] = dd > 1e-12f ? (float)((double)nv[r] / (double)den) : sv[r];
+            P.dst[(int64_t)y * P.dstride + xs + j] = dd > 1e-12f ? (float)((double)nv[j] / (double)den) : sv[j];
         }
     }
-#undef wt
-#undef hs
 }
 
 }  // namespace
 
 void launch_finish_batch(const FinishBatch& fb, cudaStream_t stream) {
     if (fb.total_ctas <= 0) return;
-    const size_t smem = (size_t)(kFY + fb.block - 1) * (kFX + fb.block - 1 + kFX) * sizeof(long long);
+    const size_t smem = (size_t)kFY * vs_pitch(fb.block) * sizeof(long long);
     auto kern = fb.block == 8 ? finish_batch_kernel<8> : finish_batch_kernel<0>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<fb.total_ctas, kFT, smem, stream>>>(fb);

@@ -235,21 +235,24 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 #pragma unroll
         for (int j = 0; j < 8; ++j) cube[g * Sh::S + row * 8 + j] = v[j];
     }
-    if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn((double)weight * kFixedScale));
+    // weight x value x 2^32 is exact in double (a 24 x 24-bit product and a
+    // power of two), so scaling the weight first rounds the same
+    const double wscaled = (double)weight * kFixedScale;
+    if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
     __syncwarp();
     // aggregation with 8 consecutive lanes on 8 consecutive pixels of a row:
-    // a warp instruction covers 4 rows x 8 columns of one patch
+    // a warp instruction covers 4 rows x 8 columns of one patch (k is the
+    // same on every lane, so the loop ends for the whole warp at once)
 #pragma unroll
-    for (int t = 0; t < 2 * G; ++t) {
-        const int e = t * 32 + lane, gg = e >> 6, i = (e >> 3) & 7, j = e & 7;
-        if (gg < k) {
-            const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
-            const int ss = __shfl_sync(0xffffffffu, s, gg * Sh::LP);
+    for (int gg = 0; gg < G; ++gg) {
+        if (gg >= k) break;
+        const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
+        const int ss = __shfl_sync(0xffffffffu, s, gg * Sh::LP);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = 4 * h + (lane >> 3), j = lane & 7;
             add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
-                    __double2ll_rn((double)weight * (double)cube[gg * Sh::S + i * 8 + j] * kFixedScale));
-        } else {
-            (void)__shfl_sync(0xffffffffu, p, 0);
-            (void)__shfl_sync(0xffffffffu, s, 0);
+                    __double2ll_rn(wscaled * (double)cube[gg * Sh::S + i * 8 + j]));
         }
     }
     __syncwarp();
@@ -287,7 +290,9 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
     }
 }
 
-// Temporal centre, batched over its planes: each plane with its own slots.
+// Temporal centre, batched over its planes: each plane with its own slots;
+// the next job's count, positions and slots are read ahead as in the
+// batched form below.
 template <int G, bool WIENER>
 __global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const __grid_constant__ GroupSlotBatch gb) {
     using Sh = Shape<G>;
@@ -297,31 +302,49 @@ __global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const _
     const int g = lane / Sh::LP;
     const int stride_w = gridDim.x * kWarps;
     int pl = 0;
-    for (int job = blockIdx.x * kWarps + warp; job < gb.total_jobs; job += stride_w) {
-        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= job) ++pl;
+    const auto fetch = [&](int jb, int& k, int32_t& p, int& s, int& plane) {
+        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= jb) ++pl;
         const GroupSlotPlane& P_ = gb.p[pl];
-        const GroupIO& io = P_.io;
-        const int lj = job - P_.job0;
-        const int k = P_.count[lj];
-        if (k <= 0) continue;
-        const int32_t p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
-        const int s = (P_.slot && g < k) ? P_.slot[(size_t)lj * G + g] : 0;
-        filter_group<G, WIENER>(
-            smem[warp], smem[warp] + CUBE, lane, k, p, s, P_.sigma,
-            [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
-            [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
-            [&](int sl, int x, int y, long long v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(io.num[sl] + (int64_t)y * io.acc_stride + x),
-                          (unsigned long long)v);
-            },
-            [&](int sl, int x, int y, long long v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
-                          (unsigned long long)v);
-            });
+        const int lj = jb - P_.job0;
+        k = P_.count[lj];
+        p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
+        s = (P_.slot && g < k) ? P_.slot[(size_t)lj * G + g] : 0;
+        plane = pl;
+    };
+    int job = blockIdx.x * kWarps + warp;
+    int k = 0, s = 0, plane = 0;
+    int32_t p = 0;
+    if (job < gb.total_jobs) fetch(job, k, p, s, plane);
+    for (; job < gb.total_jobs; job += stride_w) {
+        int kn = 0, sn = 0, plane_n = plane;
+        int32_t pn = 0;
+        if (job + stride_w < gb.total_jobs) fetch(job + stride_w, kn, pn, sn, plane_n);
+        if (k > 0) {
+            const GroupSlotPlane& P_ = gb.p[plane];
+            const GroupIO& io = P_.io;
+            filter_group<G, WIENER>(
+                smem[warp], smem[warp] + CUBE, lane, k, p, s, P_.sigma,
+                [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
+                [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
+                [&](int sl, int x, int y, long long v) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(io.num[sl] + (int64_t)y * io.acc_stride + x),
+                              (unsigned long long)v);
+                },
+                [&](int sl, int x, int y, long long v) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
+                              (unsigned long long)v);
+                });
+        }
+        k = kn;
+        s = sn;
+        p = pn;
+        plane = plane_n;
     }
 }
 
-// Batched form: every job of every plane of the batch, a warp per group.
+// Batched form: every job of every plane of the batch, a warp per group. A
+// warp reads its next job's count and positions before it filters the
+// current one, so that dependent pair of loads overlaps the transforms.
 template <int G, bool WIENER, int NW>
 __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_constant__ GroupBatch gb) {
     using Sh = Shape<G>;
@@ -331,25 +354,40 @@ __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_cons
     const int g = lane / Sh::LP;
     const int stride_w = gridDim.x * NW;
     int pl = 0;
-    for (int job = blockIdx.x * NW + warp; job < gb.total_jobs; job += stride_w) {
-        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= job) ++pl;
+    const auto fetch = [&](int jb, int& k, int32_t& p, int& plane) {
+        while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= jb) ++pl;
         const GroupPlane& P_ = gb.p[pl];
-        const int lj = job - P_.job0;
-        const int k = P_.count[lj];
-        if (k <= 0) continue;
-        const int32_t p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
-        filter_group<G, WIENER>(
-            smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma,
-            [&](int, int row) { return P_.src + (int64_t)row * P_.stride; },
-            [&](int, int row) { return P_.ref + (int64_t)row * P_.ref_stride; },
-            [&](int, int x, int y, long long v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(P_.num + (int64_t)y * P_.acc_stride + x),
-                          (unsigned long long)v);
-            },
-            [&](int, int x, int y, long long v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(P_.wsum + (int64_t)y * P_.acc_stride + x),
-                          (unsigned long long)v);
-            });
+        const int lj = jb - P_.job0;
+        k = P_.count[lj];
+        p = g < k ? P_.pos[(size_t)lj * G + g] : 0;
+        plane = pl;
+    };
+    int job = blockIdx.x * NW + warp;
+    int k = 0, plane = 0;
+    int32_t p = 0;
+    if (job < gb.total_jobs) fetch(job, k, p, plane);
+    for (; job < gb.total_jobs; job += stride_w) {
+        int kn = 0, plane_n = plane;
+        int32_t pn = 0;
+        if (job + stride_w < gb.total_jobs) fetch(job + stride_w, kn, pn, plane_n);
+        if (k > 0) {
+            const GroupPlane& P_ = gb.p[plane];
+            filter_group<G, WIENER>(
+                smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma,
+                [&](int, int row) { return P_.src + (int64_t)row * P_.stride; },
+                [&](int, int row) { return P_.ref + (int64_t)row * P_.ref_stride; },
+                [&](int, int x, int y, long long v) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(P_.num + (int64_t)y * P_.acc_stride + x),
+                              (unsigned long long)v);
+                },
+                [&](int, int x, int y, long long v) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(P_.wsum + (int64_t)y * P_.acc_stride + x),
+                              (unsigned long long)v);
+                });
+        }
+        k = kn;
+        p = pn;
+        plane = plane_n;
     }
 }
 

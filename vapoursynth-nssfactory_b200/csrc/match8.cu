@@ -9,9 +9,10 @@
 //     batch. Two lanes serve each reference, one per column half, each with
 //     its 8x4 half block in 32 registers; a warp is 16 references x 2 halves
 //     and the CTA's P warp pairs split the 2R+1 window columns;
-//   - the CTA stages the 2R+8 rows of its windows once in shared memory, the
-//     column c of a row stored at c ^ ((c >> 5) & 3): the 32 lanes read 32
-//     columns 4 apart, which this swizzle sends to 32 different banks;
+//   - the CTA stages the 2R+8 rows of its windows once in shared memory by
+//     asynchronous copies (all issued, then one wait), the column c of a row
+//     stored at c ^ ((c >> 5) & 3): the 32 lanes read 32 columns 4 apart,
+//     which this swizzle sends to 32 different banks;
 //   - a lane walks its window columns one by one: the column's 2R+8 image rows
 //     stream through and every row is applied to the 8 candidates that
 //     overlap it. Candidate k lives in accumulator k & 7; with the row loop
@@ -98,9 +99,11 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
         float* dst = tile + r * kPitch;
         for (int c = lane; c < TW; c += 32) {
             const int gx = X0 + c;
-            dst[swz(c)] = (yok && gx >= 0 && gx < W) ? __ldg(src + gx) : 0.f;
+            const bool ok = yok && gx >= 0 && gx < W;
+            cp_async4(dst + swz(c), ok ? src + gx : src, ok ? 4 : 0);
         }
     }
+    cp_async_wait_all();
     __syncthreads();
 
     const int rg = warp & 1, part = warp >> 1, half = lane >> 4;
