@@ -529,13 +529,28 @@ __global__ void __launch_bounds__(2 * kSRefs, 8) temporal8s_kernel(const __grid_
                     float2 acc[8][2];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
+                    // rows are read LA rows ahead of their use
+                    constexpr int LA = 2;
+                    float2 q01[LA], q23[LA];
+#pragma unroll
+                    for (int a = 0; a < LA; ++a) {
+                        q01[a] = q23[a] = make_float2(0.f, 0.f);
+                        if (colok && a < nk + B - 1) {
+                            const float* rowp = colp + (int64_t)a * ps;
+                            q01[a] = make_float2(__ldg(rowp), __ldg(rowp + 1));
+                            q23[a] = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
+                        }
+                    }
 #pragma unroll
                     for (int srow = 0; srow < ROWS; ++srow) {
-                        float2 p01 = make_float2(0.f, 0.f), p23 = make_float2(0.f, 0.f);
-                        if (colok && srow < nk + B - 1) {
-                            const float* rowp = colp + (int64_t)srow * ps;
-                            p01 = make_float2(__ldg(rowp), __ldg(rowp + 1));
-                            p23 = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
+                        const float2 p01 = q01[srow % LA], p23 = q23[srow % LA];
+                        if (srow + LA < ROWS) {
+                            q01[srow % LA] = q23[srow % LA] = make_float2(0.f, 0.f);
+                            if (colok && srow + LA < nk + B - 1) {
+                                const float* rowp = colp + (int64_t)(srow + LA) * ps;
+                                q01[srow % LA] = make_float2(__ldg(rowp), __ldg(rowp + 1));
+                                q23[srow % LA] = make_float2(__ldg(rowp + 2), __ldg(rowp + 3));
+                            }
                         }
 #pragma unroll
                         for (int ii = 0; ii < B; ++ii) {
