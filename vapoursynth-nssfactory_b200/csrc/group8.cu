@@ -4,8 +4,12 @@
 // per group, the cube in registers and a padded per-warp shared buffer:
 //   - 32/G lanes per patch, each holding 8G/32 rows, then as many columns,
 //     then two Haar tubes (coefficient positions l and l+32 across the group);
-//   - the per-patch stride is 64 + 32/G floats, so the column and tube
-//     phases of the 32 lanes touch 32 different banks;
+//   - the per-patch stride is 64 + 32/G floats and a coefficient's column is
+//     XORed with its row's owner lane, so the row, column and tube phases of
+//     the 32 lanes each touch 32 different banks;
+//   - the inverse runs rows first, then columns (the oracle's order); for
+//     groups of up to 8 the columns stay in registers and each lane adds its
+//     own patch's pixels to the sums from there;
 //   - the 8-point DCT-II is evaluated through its even/odd symmetry: with
 //     a_n = x_n + x_{7-n}, b_n = x_n - x_{7-n}, the even outputs are a 4-point
 //     DCT of a (split again the same way) and the odd outputs a 4x4 cosine
@@ -108,6 +112,10 @@ struct Shape {
     static constexpr int LP = 32 / G;      // lanes per patch
     static constexpr int RPL = 8 / LP;     // rows (and columns) per lane
     static constexpr int S = 64 + LP;      // patch stride in the shared cube
+    // word of coefficient (row, col) within a patch: the column is XORed
+    // with the row's owner lane (row / RPL < LP), so row, column and tube
+    // accesses of the 32 lanes each touch 32 different banks
+    __device__ static __forceinline__ int at(int row, int col) { return row * 8 + (col ^ (row / RPL)); }
 };
 
 // rows -> (DCT on rows) -> cube, cube -> columns -> (DCT) -> cube
@@ -119,13 +127,13 @@ __device__ __forceinline__ void col_pass(float* cube, int g, int q) {
         const int c = q + Sh::LP * t;
         float v[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + i * 8 + c];
+        for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + Sh::at(i, c)];
         if (INV)
             idct8(v);
         else
             fdct8(v);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) cube[g * Sh::S + i * 8 + c] = v[i];
+        for (int i = 0; i < 8; ++i) cube[g * Sh::S + Sh::at(i, c)] = v[i];
     }
 }
 
@@ -158,11 +166,11 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         }
         fdct8(v);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) cube[g * Sh::S + row * 8 + j] = v[j];
+        for (int j = 0; j < 8; ++j) cube[g * Sh::S + Sh::at(row, j)] = v[j];
         if (WIENER) {
             fdct8(w);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) rcube[g * Sh::S + row * 8 + j] = w[j];
+            for (int j = 0; j < 8; ++j) rcube[g * Sh::S + Sh::at(row, j)] = w[j];
         }
     }
     __syncwarp();
@@ -174,15 +182,15 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
     float w2 = 0.f;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        const int f = lane + 32 * h;
+        const int f = lane + 32 * h, fa = Sh::at(f >> 3, f & 7);
         float t[G];
 #pragma unroll
-        for (int gg = 0; gg < G; ++gg) t[gg] = cube[gg * Sh::S + f];
+        for (int gg = 0; gg < G; ++gg) t[gg] = cube[gg * Sh::S + fa];
         haar_fwd<G>(t);
         if (WIENER) {
             float r[G];
 #pragma unroll
-            for (int gg = 0; gg < G; ++gg) r[gg] = rcube[gg * Sh::S + f];
+            for (int gg = 0; gg < G; ++gg) r[gg] = rcube[gg * Sh::S + fa];
             haar_fwd<G>(r);
             const float sig2 = sigma * sigma;
 #pragma unroll
@@ -209,7 +217,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         }
         haar_inv<G>(t);
 #pragma unroll
-        for (int gg = 0; gg < G; ++gg) cube[gg * Sh::S + f] = t[gg];
+        for (int gg = 0; gg < G; ++gg) cube[gg * Sh::S + fa] = t[gg];
     }
     float weight;
     if (WIENER) {
@@ -221,38 +229,68 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
         weight = __fdiv_rn(1.f, (float)(kept > 1 ? kept : 1));
     }
-    __syncwarp();
-    col_pass<G, true>(cube, g, q);
-    __syncwarp();
-    // inverse row transforms back into the cube
-#pragma unroll
-    for (int r = 0; r < Sh::RPL; ++r) {
-        const int row = q * Sh::RPL + r;
-        float v[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + row * 8 + j];
-        idct8(v);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) cube[g * Sh::S + row * 8 + j] = v[j];
-    }
     // weight x value x 2^32 is exact in double (a 24 x 24-bit product and a
     // power of two), so scaling the weight first rounds the same
     const double wscaled = (double)weight * kFixedScale;
-    if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
     __syncwarp();
-    // aggregation with 8 consecutive lanes on 8 consecutive pixels of a row:
-    // a warp instruction covers 4 rows x 8 columns of one patch (k is the
-    // same on every lane, so the loop ends for the whole warp at once)
+    if constexpr (G <= 8) {
+        // inverse rows in the cube, then inverse columns kept in registers and
+        // added from there: lane (g, q) holds columns q + LP t of its own
+        // patch, so the LP lanes of a patch add LP adjacent pixels of a row
 #pragma unroll
-    for (int gg = 0; gg < G; ++gg) {
-        if (gg >= k) break;
-        const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
-        const int ss = __shfl_sync(0xffffffffu, s, gg * Sh::LP);
+        for (int r = 0; r < Sh::RPL; ++r) {
+            const int row = q * Sh::RPL + r;
+            float v[8];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = 4 * h + (lane >> 3), j = lane & 7;
-            add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
-                    __double2ll_rn(wscaled * (double)cube[gg * Sh::S + i * 8 + j]));
+            for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + Sh::at(row, j)];
+            idct8(v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) cube[g * Sh::S + Sh::at(row, j)] = v[j];
+        }
+        __syncwarp();
+        if (g < k) {
+            if (q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
+#pragma unroll
+            for (int t = 0; t < Sh::RPL; ++t) {
+                const int c = q + Sh::LP * t;
+                float v[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + Sh::at(i, c)];
+                idct8(v);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) add_num(s, px + c, py + i, __double2ll_rn(wscaled * (double)v[i]));
+            }
+        }
+    } else {
+        // groups of 16 (two lanes per patch): inverse columns, inverse rows,
+        // then 8 consecutive lanes on 8 consecutive pixels of a row, a warp
+        // instruction covering 4 rows of one patch (k is the same on every
+        // lane, so the loop ends for the whole warp at once)
+        col_pass<G, true>(cube, g, q);
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < Sh::RPL; ++r) {
+            const int row = q * Sh::RPL + r;
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = cube[g * Sh::S + Sh::at(row, j)];
+            idct8(v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) cube[g * Sh::S + Sh::at(row, j)] = v[j];
+        }
+        if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
+        __syncwarp();
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg) {
+            if (gg >= k) break;
+            const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
+            const int ss = __shfl_sync(0xffffffffu, s, gg * Sh::LP);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = 4 * h + (lane >> 3), j = lane & 7;
+                add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
+                        __double2ll_rn(wscaled * (double)cube[gg * Sh::S + Sh::at(i, j)]));
+            }
         }
     }
     __syncwarp();
