@@ -113,13 +113,38 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
     // output mapping: row r of the tile, pixels 8 * seg .. 8 * seg + 7
     const int r = threadIdx.x >> 3, seg = threadIdx.x & 7;
     const int y = y0 + r, xs = x0 + 8 * seg;
+    // a full segment of 16-byte aligned rows moves as vectors
+    const bool vec = y < P.H && xs + 8 <= P.W &&
+                     ((reinterpret_cast<uintptr_t>(P.num) | reinterpret_cast<uintptr_t>(P.src) |
+                       reinterpret_cast<uintptr_t>(P.dst)) & 15) == 0 &&
+                     ((P.acc_stride | P.sstride | P.dstride) & 3) == 0;
+    long long* const np = P.num + (int64_t)y * P.acc_stride + xs;
+    float* const dp = P.dst + (int64_t)y * P.dstride + xs;
     long long nv[8];
     float sv[8];
+    if (vec) {
+        const float* sp = P.src + (int64_t)y * P.sstride + xs;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const bool ok = xs + j < P.W && y < P.H;
-        nv[j] = ok ? P.num[(int64_t)y * P.acc_stride + xs + j] : 0;
-        sv[j] = ok ? __ldg(P.src + (int64_t)y * P.sstride + xs + j) : 0.f;
+        for (int h = 0; h < 4; ++h) {
+            const longlong2 t = reinterpret_cast<const longlong2*>(np)[h];
+            nv[2 * h] = t.x;
+            nv[2 * h + 1] = t.y;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(sp) + h);
+            sv[4 * h] = t.x;
+            sv[4 * h + 1] = t.y;
+            sv[4 * h + 2] = t.z;
+            sv[4 * h + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const bool ok = xs + j < P.W && y < P.H;
+            nv[j] = ok ? np[j] : 0;
+            sv[j] = ok ? __ldg(P.src + (int64_t)y * P.sstride + xs + j) : 0.f;
+        }
     }
     // vertical sums: quarter q, tile column c (vs column c + B - 1) and, for
     // c < B - 1, halo column c (vs column c)
@@ -169,13 +194,26 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
     const long long* row = vs + r * pitch;
     long long den = 0;
     for (int k = 0; k < B; ++k) den += row[vs_col(8 * seg + k)];
+    float out[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         if (j > 0) den += row[vs_col(8 * seg + j + B - 1)] - row[vs_col(8 * seg + j - 1)];
-        if (xs + j < P.W && y < P.H) {
-            P.num[(int64_t)y * P.acc_stride + xs + j] = 0;
-            const float dd = (float)((double)den * kFixedInv);
-            P.dst[(int64_t)y * P.dstride + xs + j] = dd > 1e-12f ? (float)((double)nv[j] / (double)den) : sv[j];
+        const float dd = (float)((double)den * kFixedInv);
+        out[j] = dd > 1e-12f ? (float)((double)nv[j] / (double)den) : sv[j];
+    }
+    if (vec) {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) reinterpret_cast<longlong2*>(np)[h] = make_longlong2(0, 0);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            reinterpret_cast<float4*>(dp)[h] = make_float4(out[4 * h], out[4 * h + 1], out[4 * h + 2], out[4 * h + 3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (xs + j < P.W && y < P.H) {
+                np[j] = 0;
+                dp[j] = out[j];
+            }
         }
     }
 }
