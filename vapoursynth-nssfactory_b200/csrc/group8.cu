@@ -137,12 +137,34 @@ __device__ __forceinline__ void col_pass(float* cube, int g, int q) {
     }
 }
 
+// Eight consecutive floats of a row starting at any column: from 16-byte
+// aligned rows (vec) as the two or three aligned 16-byte chunks covering
+// them (a chunk holding a valid float never leaves its allocation), else
+// one float at a time.
+__device__ __forceinline__ void load_row8(const float* rowp, int px, bool vec, float (&v)[8]) {
+    if (vec) {
+        const int o = px & 3;
+        const float4* a = reinterpret_cast<const float4*>(rowp + (px - o));
+        const float4 c0 = __ldg(a), c1 = __ldg(a + 1);
+        const float4 c2 = o != 0 ? __ldg(a + 2) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float w[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = o == 0 ? w[j] : o == 1 ? w[j + 1] : o == 2 ? w[j + 2] : w[j + 3];
+    } else {
+        const float* sp = rowp + px;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = __ldg(sp + j);
+    }
+}
+
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 // One group on one warp. Acc(s) gives the (num, wsum, stride) of slot s,
 // Src(s, row, x) / Ref(s, row, x) the source rows.
 template <int G, bool WIENER, class SrcRow, class RefRow, class AddNum, class AddWeight>
 __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane, int k, int32_t p, int s,
-                                             float sigma, SrcRow src_row, RefRow ref_row, AddNum add_num,
-                                             AddWeight add_weight) {
+                                             float sigma, bool vec, SrcRow src_row, RefRow ref_row,
+                                             AddNum add_num, AddWeight add_weight) {
     using Sh = Shape<G>;
     const int g = lane / Sh::LP, q = lane % Sh::LP;
     const int px = pos_x(p), py = pos_y(p);
@@ -152,14 +174,8 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         const int row = q * Sh::RPL + r;
         float v[8], w[8];
         if (g < k) {
-            const float* sp = src_row(s, py + row) + px;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = __ldg(sp + j);
-            if (WIENER) {
-                const float* rp = ref_row(s, py + row) + px;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) w[j] = __ldg(rp + j);
-            }
+            load_row8(src_row(s, py + row), px, vec, v);
+            if (WIENER) load_row8(ref_row(s, py + row), px, vec, w);
         } else {
 #pragma unroll
             for (int j = 0; j < 8; ++j) v[j] = w[j] = 0.f;
@@ -308,13 +324,15 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / Sh::LP;
     const int stride_w = gridDim.x * kWarps;
+    bool vec = io.stride % 4 == 0 && io.ref_stride % 4 == 0;
+    for (int q = 0; q < kMaxSlots; ++q) vec = vec && aligned16(io.src[q]) && aligned16(io.ref[q]);
     for (int job = blockIdx.x * kWarps + warp; job < njobs; job += stride_w) {
         const int k = count[job];
         if (k <= 0) continue;
         const int32_t p = g < k ? pos[(size_t)job * G + g] : 0;
         const int s = (slot && g < k) ? slot[(size_t)job * G + g] : 0;
         filter_group<G, WIENER>(
-            smem[warp], smem[warp] + CUBE, lane, k, p, s, sigma,
+            smem[warp], smem[warp] + CUBE, lane, k, p, s, sigma, vec,
             [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
             [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
             [&](int sl, int x, int y, long long v) {
@@ -339,6 +357,14 @@ __global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const _
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / Sh::LP;
     const int stride_w = gridDim.x * kWarps;
+    // planes whose every slot row is 16-byte aligned
+    int vec_mask = 0;
+    for (int q = 0; q < gb.n; ++q) {
+        const GroupIO& io = gb.p[q].io;
+        bool vec = io.stride % 4 == 0 && io.ref_stride % 4 == 0;
+        for (int t = 0; t < kMaxSlots; ++t) vec = vec && aligned16(io.src[t]) && aligned16(io.ref[t]);
+        vec_mask |= int(vec) << q;
+    }
     int pl = 0;
     const auto fetch = [&](int jb, int& k, int32_t& p, int& s, int& plane) {
         while (pl + 1 < gb.n && gb.p[pl + 1].job0 <= jb) ++pl;
@@ -361,7 +387,7 @@ __global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const _
             const GroupSlotPlane& P_ = gb.p[plane];
             const GroupIO& io = P_.io;
             filter_group<G, WIENER>(
-                smem[warp], smem[warp] + CUBE, lane, k, p, s, P_.sigma,
+                smem[warp], smem[warp] + CUBE, lane, k, p, s, P_.sigma, (vec_mask >> plane) & 1,
                 [&](int sl, int row) { return io.src[sl] + (int64_t)row * io.stride; },
                 [&](int sl, int row) { return io.ref[sl] + (int64_t)row * io.ref_stride; },
                 [&](int sl, int x, int y, long long v) {
@@ -410,8 +436,9 @@ __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_cons
         if (job + stride_w < gb.total_jobs) fetch(job + stride_w, kn, pn, plane_n);
         if (k > 0) {
             const GroupPlane& P_ = gb.p[plane];
+            const bool vec = P_.stride % 4 == 0 && P_.ref_stride % 4 == 0 && aligned16(P_.src) && aligned16(P_.ref);
             filter_group<G, WIENER>(
-                smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma,
+                smem[warp], smem[warp] + CUBE, lane, k, p, 0, P_.sigma, vec,
                 [&](int, int row) { return P_.src + (int64_t)row * P_.stride; },
                 [&](int, int row) { return P_.ref + (int64_t)row * P_.ref_stride; },
                 [&](int, int x, int y, long long v) {
