@@ -44,15 +44,16 @@ struct TopK {
 #pragma unroll
         for (int q = 0; q < K; ++q) k[q] = ~0ull;
     }
+    // all K comparisons first (independent), then every slot takes its own
+    // entry, the one before it, or v: no chain through the list
     __device__ __forceinline__ void add(uint64_t v) {
         if (!(v < k[K - 1])) return;
+        bool c[K];
 #pragma unroll
-        for (int q = 0; q < K; ++q) {
-            const uint64_t a = k[q];
-            const bool s = v < a;
-            k[q] = s ? v : a;
-            v = s ? a : v;
-        }
+        for (int q = 0; q < K; ++q) c[q] = v < k[q];
+#pragma unroll
+        for (int q = K - 1; q > 0; --q) k[q] = c[q] ? (c[q - 1] ? k[q - 1] : v) : k[q];
+        k[0] = c[0] ? v : k[0];
     }
 };
 

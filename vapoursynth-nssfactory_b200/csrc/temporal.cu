@@ -215,15 +215,16 @@ struct LaneTop {
 #pragma unroll
         for (int q = 0; q < PS; ++q) k[q] = ~0ull;
     }
+    // all comparisons first, then each slot takes its own entry, the one
+    // before it, or v (no dependency chain through the list)
     __device__ __forceinline__ void add(uint64_t v) {
         if (!(v < k[PS - 1])) return;
+        bool c[PS];
 #pragma unroll
-        for (int q = 0; q < PS; ++q) {
-            const uint64_t a = k[q];
-            const bool sw = v < a;
-            k[q] = sw ? v : a;
-            v = sw ? a : v;
-        }
+        for (int q = 0; q < PS; ++q) c[q] = v < k[q];
+#pragma unroll
+        for (int q = PS - 1; q > 0; --q) k[q] = c[q] ? (c[q - 1] ? k[q - 1] : v) : k[q];
+        k[0] = c[0] ? v : k[0];
     }
     __device__ __forceinline__ void pop() {
 #pragma unroll
