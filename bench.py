@@ -16,7 +16,7 @@ is read cold.
   bits.
 - e2e: the batched call on pinned host frames: the host->device copy of each
   frame and the device->host copy of its result are inside the timed region
-  (chunks on two streams overlap copies and kernels).
+  (chunks on three streams overlap copies and kernels).
 - roofline: the dominant kernel (exact FP32 matcher), algorithmic flops
   (3 * B^2 per reference-candidate pair) over its event-timed duration,
   against the FP32 SIMT peak (148 SMs x 128 lanes x 2 flops x clock).

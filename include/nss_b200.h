@@ -249,7 +249,7 @@ typedef struct nssb_batch_info {
 } nssb_batch_info;
 /* args (ints): "autotune" (default 1), "graph" (default 1), "chunk_frames"
  * (frames per chunk; default 0: one chunk when every item is on the device,
- * else up to six equal chunks on two streams so that host copies overlap
+ * else up to ten equal chunks on three streams so that host copies overlap
  * the kernels), and the shapes
  * used when autotune is 0: "match_form" (0 FP32, 1 tensor-core precision
  * form; default 0), "match_parts" (1, 2, 4; default 2),

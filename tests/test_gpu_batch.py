@@ -99,7 +99,7 @@ def test_mixed_batch_equals_per_frame(nssb, nodes):
 
 @pytest.mark.parametrize("chunk", [0, 1, 4])
 def test_chunked_two_stream_runs(nssb, nodes, chunk):
-    # host items split into chunks on two streams (0: automatic), repeated
+    # host items split into chunks on three streams (0: automatic), repeated
     reqs = [(n, f) for f in (0, 1) for n in nodes]
     want = expected(nodes, reqs)
     b = nssb.Batch(chunk_frames=chunk)

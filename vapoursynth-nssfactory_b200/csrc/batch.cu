@@ -406,10 +406,10 @@ BatchPlan& BatchEngine::plan_for(const std::string& sig, int lane) {
     return *plans_.back().second;
 }
 
-constexpr int kMaxChunks = 6, kMinChunkFrames = 4;
+constexpr int kMaxChunks = 10, kMinChunkFrames = 3;
 
 // Chunks of the batch: one when every item is on the device (nothing to
-// overlap), else up to six equal chunks so that the host copies of one
+// overlap), else up to ten equal chunks so that the host copies of one
 // chunk overlap the kernels of its neighbours.
 std::vector<std::pair<int, int>> BatchEngine::chunks(const BatchItem* items, int n) const {
     bool host = false;
@@ -452,7 +452,7 @@ void BatchEngine::run(const BatchItem* items, int n) {
     bool started = false;
     try {
         for (size_t k = 0; k < parts.size(); ++k) {
-            const int lane = (int)(k % 2);
+            const int lane = (int)(k % kLanes);
             cudaStream_t s = streams_[lane];
             const BatchItem* c = items + parts[k].first;
             const int m = parts[k].second;
@@ -467,7 +467,7 @@ void BatchEngine::run(const BatchItem* items, int n) {
             }
             if (!started) {
                 NSSB_CUDA(cudaEventRecord(t0_, streams_[0]));
-                NSSB_CUDA(cudaStreamWaitEvent(streams_[1], t0_, 0));
+                for (int l = 1; l < kLanes; ++l) NSSB_CUDA(cudaStreamWaitEvent(streams_[l], t0_, 0));
                 started = true;
             }
             if (!need_tune) plan.upload(c, m, s);
@@ -482,17 +482,20 @@ void BatchEngine::run(const BatchItem* items, int n) {
             plan.download(c, m, s);
             last = t;
         }
-        for (int l = 0; l < 2; ++l) NSSB_CUDA(cudaEventRecord(t1_[l], streams_[l]));
+        for (int l = 0; l < kLanes; ++l) NSSB_CUDA(cudaEventRecord(t1_[l], streams_[l]));
         for (auto& st : streams_) NSSB_CUDA(cudaStreamSynchronize(st));
     } catch (...) {
         for (auto& st : streams_) (void)cudaStreamSynchronize(st);
         plans_.clear();  // sums may be left mid-stage: lay out afresh
         throw;
     }
-    float ms0 = 0.f, ms1 = 0.f;
-    NSSB_CUDA(cudaEventElapsedTime(&ms0, t0_, t1_[0]));
-    NSSB_CUDA(cudaEventElapsedTime(&ms1, t0_, t1_[1]));
-    info_.last_run_ms = std::max(ms0, ms1);
+    float ms = 0.f;
+    for (int l = 0; l < kLanes; ++l) {
+        float m = 0.f;
+        NSSB_CUDA(cudaEventElapsedTime(&m, t0_, t1_[l]));
+        ms = std::max(ms, m);
+    }
+    info_.last_run_ms = ms;
     info_.kernel_launches = launches;
     info_.chunks = (int)parts.size();
     info_.match_parts = last.match.parts;

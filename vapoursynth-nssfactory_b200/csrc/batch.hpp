@@ -125,8 +125,12 @@ private:
     std::vector<std::pair<int, int>> chunks(const BatchItem* items, int n) const;
     int device_;
     BatchOptions opt_;
-    cudaStream_t streams_[2] = {nullptr, nullptr};
-    cudaEvent_t t0_ = nullptr, t1_[2] = {nullptr, nullptr};
+    // chunks rotate over kLanes streams: a chunk's download and the upload
+    // of the chunk after next on the same stream hide behind the kernels of
+    // the chunks between them
+    static constexpr int kLanes = 3;
+    cudaStream_t streams_[kLanes] = {};
+    cudaEvent_t t0_ = nullptr, t1_[kLanes] = {};
     std::vector<std::pair<std::string, std::unique_ptr<BatchPlan>>> plans_;  // least recently used first
     std::map<std::string, LaunchTunes> tuned_;
     std::mutex mu_;
