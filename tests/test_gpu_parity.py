@@ -52,7 +52,9 @@ def gpu_match(nssb, plane_np, block, step, rng_, group, dev):
 SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 7), (12, 6, 8, 5),
           (2, 2, 4, 4), (1, 1, 2, 3), (32, 16, 4, 3), (8, 3, 64, 7), (8, 8, 1, 9), (4, 3, 16, 12),
           # the 8x8 fast path at its other ranges
-          (8, 8, 8, 4), (8, 8, 16, 5), (8, 5, 4, 6), (8, 8, 8, 7), (8, 2, 2, 8), (8, 6, 8, 12), (8, 8, 16, 15)]
+          (8, 8, 8, 4), (8, 8, 16, 5), (8, 5, 4, 6), (8, 8, 8, 7), (8, 2, 2, 8), (8, 6, 8, 12), (8, 8, 16, 15),
+          # large windows (bm_range 25 and up: the window spans most of the test image)
+          (8, 8, 8, 25), (8, 4, 16, 32), (4, 3, 8, 40), (16, 8, 8, 64)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", SHAPES)
@@ -106,7 +108,7 @@ def gpu_stage(nssb, src, ref, st, dev):
 
 
 STAGES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (16, 8, 16, 7), (12, 6, 8, 5), (2, 2, 4, 4), (1, 1, 2, 3),
-          (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4)]
+          (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4), (8, 8, 16, 25), (8, 4, 8, 32)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", STAGES)
