@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--served", type=int, default=2000, help="requests of the serving leg (0: skip it)")
-    ap.add_argument("--no-legs", action="store_true", help="skip the temporal (C3) and mixed-batch (C4) legs")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the temporal (C3), mixed-batch (C4) and served legs (profiling runs)")
     ap.add_argument("--served-workers", type=int, default=8, help="temporal requests the server runs at once")
     ap.add_argument("--c3-frames", type=int, default=60)
     ap.add_argument("--only", choices=["c3", "c4", "served"], help="run one leg alone (profiling)")
@@ -350,7 +351,7 @@ def our_arm(args):
     if not args.no_legs:
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
         out["batched_c4"] = c4_leg(nssb, synth, dev)
-    if args.served > 0:
+    if args.served > 0 and not args.no_legs:
         out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
                                    args.served_workers)
         out["served"]["workers"] = args.served_workers

@@ -73,7 +73,8 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
         gb.total_jobs += jobs;
     }
     clock.begin(StageClock::kOther);
-    clear_wsum_kernel<<<dim3(64, gb.n), 256, 0, stream>>>(gb);
+    // about four CTAs per SM over all planes of the set (rows grid-strided)
+    clear_wsum_kernel<<<dim3(std::max(8, std::min(512, ceil_div(592, gb.n))), gb.n), 256, 0, stream>>>(gb);
     NSSB_CUDA(cudaGetLastError());
     clock.end(StageClock::kOther);
     bool gok = false;
