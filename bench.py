@@ -351,6 +351,13 @@ def our_arm(args):
     if not args.no_legs:
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
         out["batched_c4"] = c4_leg(nssb, synth, dev)
+    # the headline's batch layouts and nodes are released before the served
+    # leg sizes its memory budget from the device's free memory
+    batch.close()
+    node_d.close()
+    node_h.close()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     if args.served > 0 and not args.no_legs:
         out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
                                    args.served_workers)
@@ -367,9 +374,6 @@ def our_arm(args):
         out["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                                "sample": f"{done} of the workload's frames, frame-parallel, {el:.1f} s; CPU "
                                          "restatement of nss.BM3D (oracle/), not the reference binary"}
-    batch.close()
-    node_d.close()
-    node_h.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
     if pg is not None:
