@@ -198,8 +198,9 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         if (j > 0) den += row[vs_col(8 * seg + j + B - 1)] - row[vs_col(8 * seg + j - 1)];
-        const float dd = (float)((double)den * kFixedInv);
-        out[j] = dd > 1e-12f ? (float)((double)nv[j] / (double)den) : sv[j];
+        // den > 1e-12 in real units is den >= 1 in units of 2^-32 (the
+        // smallest positive den, 2^-32 = 2.3e-10, already passes)
+        out[j] = den > 0 ? (float)((double)nv[j] / (double)den) : sv[j];
     }
     if (vec) {
 #pragma unroll
