@@ -67,6 +67,12 @@ void dev_free(void* p) {
     (void)cudaFreeAsync(p, device_pool(dev).stream);
 }
 
+void dev_pool_trim(int dev) {
+    DevicePool& d = device_pool(dev);
+    NSSB_CUDA(cudaStreamSynchronize(d.stream));  // frees queued on the pool's stream have landed
+    NSSB_CUDA(cudaMemPoolTrimTo(d.pool, 0));
+}
+
 namespace {
 
 int64_t pitch_of(int w) { return (int64_t)((w + 31) / 32) * 32; }

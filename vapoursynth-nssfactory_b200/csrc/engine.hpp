@@ -136,8 +136,11 @@ private:
 void plane_stage_noalloc(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,
                          const StageParams& sp, cudaStream_t stream);
 
-// Device memory helpers (cudaMalloc'd, recorded for release).
+// Device memory helpers: the library's stream-ordered pool (see dev_alloc).
 void* dev_alloc(size_t bytes);
 void dev_free(void* p);
+// Returns to the device what the library's pool on device dev keeps from
+// freed blocks (so cudaMemGetInfo counts it as free again).
+void dev_pool_trim(int dev);
 
 }  // namespace nssb

@@ -48,6 +48,9 @@ double frame_mpx(const Bm3dConfig& c) {
 Server::Server(int device, const ServerOptions& opt) : device_(device), opt_(opt) {
     NSSB_CUDA(cudaSetDevice(device_));
     if (opt_.budget_bytes == 0) {
+        // what the library's pool keeps from earlier work goes back first, so
+        // the free memory measured includes it
+        dev_pool_trim(device_);
         size_t free_b = 0, total_b = 0;
         NSSB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         opt_.budget_bytes = free_b / 10 * 8;
