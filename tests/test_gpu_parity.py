@@ -53,8 +53,10 @@ SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 
           (2, 2, 4, 4), (1, 1, 2, 3), (32, 16, 4, 3), (8, 3, 64, 7), (8, 8, 1, 9), (4, 3, 16, 12),
           # the 8x8 fast path at its other ranges
           (8, 8, 8, 4), (8, 8, 16, 5), (8, 5, 4, 6), (8, 8, 8, 7), (8, 2, 2, 8), (8, 6, 8, 12), (8, 8, 16, 15),
-          # large windows (bm_range 25 and up: the window spans most of the test image)
-          (8, 8, 8, 25), (8, 4, 16, 32), (4, 3, 8, 40), (16, 8, 8, 64)]
+          # large windows (bm_range 16 and up: the window spans most of the test image);
+          # the 8x8 fast path covers 16 and 25
+          (8, 8, 8, 25), (8, 4, 4, 25), (8, 8, 16, 16), (8, 6, 2, 16), (8, 4, 16, 32), (4, 3, 8, 40),
+          (16, 8, 8, 64)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", SHAPES)
@@ -71,6 +73,17 @@ def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_)
         bx, by = min((j % nx) * step, 61 - block), min((j // nx) * step, 47 - block)
         om = oracle.spatial_match(noisy, bx, by, block, rng_, group)
         assert [m[3] for m in om] == [float(v) for v in dist[j, :len(om)]]
+
+
+@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16)])
+def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group):
+    # windows well inside a larger plane (most references see the whole window)
+    noisy, _ = synth.gray_frame(17, 256, 160, sigma=10)
+    pos, dist, cnt = gpu_match(nssb, noisy, block=8, step=8, rng_=rng_, group=group, dev=dev)
+    st = oracle.stage(oracle.effective_sigma(10.0), block=8, group=group, step=8, bm_range=rng_)
+    _, want, wcnt = oracle.bm3d_plane(noisy, st, want_matches=True)
+    assert np.array_equal(cnt, wcnt)
+    assert np.array_equal(pos, want)
 
 
 def test_match_exact_ties(nssb, oracle, dev):
@@ -108,7 +121,8 @@ def gpu_stage(nssb, src, ref, st, dev):
 
 
 STAGES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (16, 8, 16, 7), (12, 6, 8, 5), (2, 2, 4, 4), (1, 1, 2, 3),
-          (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4), (8, 8, 16, 25), (8, 4, 8, 32)]
+          (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4), (8, 8, 16, 25), (8, 4, 8, 32),
+          (8, 8, 8, 16)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", STAGES)

@@ -1,5 +1,5 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape
-// (bm_range 9), and the ranges 4-9, 12 and 15.
+// (bm_range 9), and the ranges 4-9, 12, 15, 16 and 25.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
 // keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
@@ -25,6 +25,7 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace nssb {
 namespace {
@@ -58,10 +59,21 @@ struct TopK {
 };
 
 constexpr int kLanes = 32;   // references per CTA
-constexpr int kPitch = 288;  // tile row pitch: >= 31 * 8 + 2 * 9 + 8 columns
+// tile row pitch: the 31 * 8 + 2R + 8 columns of 32 references at step <= 8,
+// rounded up to whole 32-column groups (288 for ranges up to 15)
+template <int R>
+__host__ __device__ constexpr int tile_pitch() { return (31 * 8 + 2 * R + 8 + 31) / 32 * 32; }
 
 template <int R>
 __host__ __device__ constexpr int tile_rows() { return 2 * R + 8; }
+
+// one bit per candidate row of a window column: 32 bits up to range 15,
+// 64 up to range 31
+template <int R>
+using RowMask = typename std::conditional<(2 * R + 1 <= 32), uint32_t, uint64_t>::type;
+
+__device__ __forceinline__ int first_bit(uint32_t m) { return __ffs(m) - 1; }
+__device__ __forceinline__ int first_bit(uint64_t m) { return __ffsll((long long)m) - 1; }
 
 // Resident CTAs per SM the launch bounds ask for: 16 warps of 127 registers.
 template <int K, int P>
@@ -73,6 +85,8 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     constexpr int B = 8, HB = 4;
     constexpr int NC = 2 * R + 1;            // candidates per window column
     constexpr int TR = tile_rows<R>();
+    constexpr int kPitch = tile_pitch<R>();
+    using Mask = RowMask<R>;
     constexpr int CPW = (NC + P - 1) / P;    // window columns per warp pair
     int pl = 0;
     {
@@ -131,7 +145,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     // an emit stores its sum and marks a bit when it may enter the list; the
     // insertions run after the column, once per marked candidate
     float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
-    const uint32_t rows_ok = ((1u << (kmax + 1)) - 1u) & ~((1u << kmin) - 1u);
+    const Mask rows_ok = ((Mask(1) << (kmax + 1)) - 1) & ~((Mask(1) << kmin) - 1);
     const float2 neg1 = make_float2(-1.f, -1.f);
     // this part's columns, walked outwards from the window centre so the
     // closest candidates (usually the best) fill the list first
@@ -141,7 +155,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
         const int dxi = down ? d1 - 1 - m : d0 + m;
         const int x = cx - R + dxi;
         const bool xok = x >= left && x <= right;
-        uint32_t pass = 0;
+        Mask pass = 0;
         // a candidate may enter unless it is farther than the current worst
         // (NaN never compares greater: non-finite sums always take the exact path)
         const float worst = __uint_as_float(uint32_t(topk.k[K - 1] >> 32));
@@ -175,13 +189,13 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
                 const float half_sum = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
                 const float dd = __fadd_rn(half_sum, __shfl_xor_sync(0xffffffffu, half_sum, 16));
                 stash[kd * (64 * P)] = dd;
-                pass |= (dd > worst ? 0u : 1u) << kd;
+                pass |= Mask(dd > worst ? 0 : 1) << kd;
             }
         }
-        pass &= xok ? rows_ok : 0u;
-        if (dxi == R) pass &= ~(1u << R);
+        pass &= xok ? rows_ok : Mask(0);
+        if (dxi == R) pass &= ~(Mask(1) << R);
         while (pass) {
-            const int kd = __ffs(pass) - 1;
+            const int kd = first_bit(pass);
             pass &= pass - 1;
             topk.add(key_of(stash[kd * (64 * P)], x, cy - R + kd));
         }
@@ -254,8 +268,8 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
     mb.total_ctas = ctas;
     mb.queue = nullptr;
     if (ctas == 0) return;
-    static_assert(31 * 8 + 2 * R + 8 <= kPitch, "tile pitch too small for this range");
-    const size_t smem = std::max((size_t)(kPitch * tile_rows<R>() + (2 * R + 1) * 64 * P) * sizeof(float),
+    static_assert(2 * R + 1 <= 64, "a column's candidates must fit the row mask");
+    const size_t smem = std::max((size_t)(tile_pitch<R>() * tile_rows<R>() + (2 * R + 1) * 64 * P) * sizeof(float),
                                  (size_t)P * K * kLanes * sizeof(uint64_t));
     auto kern = match8_kernel<R, K, P>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -307,7 +321,8 @@ bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t s
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8) return false;
     const MatchTune t = tune ? *tune : MatchTune{};
-    // ranges up to 15: a column's 2R + 1 candidates fit the 32-bit pass mask
+    // the instantiated ranges; a column's 2R + 1 candidates take one bit each
+    // of a 32- or 64-bit pass mask
     switch (bm_range) {
         case 4: return launch_r<4>(mb, group, t, stream);
         case 5: return launch_r<5>(mb, group, t, stream);
@@ -317,6 +332,8 @@ bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t s
         case 9: return launch_r<9>(mb, group, t, stream);
         case 12: return launch_r<12>(mb, group, t, stream);
         case 15: return launch_r<15>(mb, group, t, stream);
+        case 16: return launch_r<16>(mb, group, t, stream);
+        case 25: return launch_r<25>(mb, group, t, stream);
         default: return false;
     }
 }
