@@ -53,8 +53,12 @@ SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 
           (2, 2, 4, 4), (1, 1, 2, 3), (32, 16, 4, 3), (8, 3, 64, 7), (8, 8, 1, 9), (4, 3, 16, 12),
           # the 8x8 fast path at its other ranges
           (8, 8, 8, 4), (8, 8, 16, 5), (8, 5, 4, 6), (8, 8, 8, 7), (8, 2, 2, 8), (8, 6, 8, 12), (8, 8, 16, 15),
+          # ranges served by the kernel of the next larger built range (10-11 on 12,
+          # 13-14 on 15, 17-24 on 25, 26-31 on 31)
+          (8, 8, 8, 10), (8, 5, 4, 11), (8, 8, 16, 13), (8, 7, 8, 20), (8, 8, 2, 24), (8, 8, 8, 28),
+          (8, 4, 16, 31),
           # large windows (bm_range 16 and up: the window spans most of the test image);
-          # the 8x8 fast path covers 16 and 25
+          # the 8x8 fast path covers up to 31
           (8, 8, 8, 25), (8, 4, 4, 25), (8, 8, 16, 16), (8, 6, 2, 16), (8, 4, 16, 32), (4, 3, 8, 40),
           (16, 8, 8, 64)]
 
@@ -75,7 +79,7 @@ def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_)
         assert [m[3] for m in om] == [float(v) for v in dist[j, :len(om)]]
 
 
-@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16)])
+@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16), (20, 8), (30, 4), (11, 8)])
 def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group):
     # windows well inside a larger plane (most references see the whole window)
     noisy, _ = synth.gray_frame(17, 256, 160, sigma=10)

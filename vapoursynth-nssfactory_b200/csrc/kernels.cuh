@@ -28,6 +28,7 @@ struct MatchPlane {
 };
 struct MatchBatch {
     int n, step;
+    int range;         // the search range (set by the 8x8 launcher; may be below the kernel's built range)
     int total_ctas;    // tiles of the launch (set by the launcher)
     int* queue;        // persistent form: next-tile counter, else null (set by the launcher)
     MatchPlane p[kMaxBatchPlanes];

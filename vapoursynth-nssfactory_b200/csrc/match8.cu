@@ -1,5 +1,6 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape
-// (bm_range 9), and the ranges 4-9, 12, 15, 16 and 25.
+// (bm_range 9), and every range from 4 to 31 (kernels built for 4-9, 12,
+// 15, 16, 25 and 31; a range between two runs on the larger one).
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
 // keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
@@ -87,7 +88,6 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     constexpr int TR = tile_rows<R>();
     constexpr int kPitch = tile_pitch<R>();
     using Mask = RowMask<R>;
-    constexpr int CPW = (NC + P - 1) / P;    // window columns per warp pair
     int pl = 0;
     {
         int lo = 0, hi = mb.n - 1;
@@ -126,8 +126,11 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     const int rx = rx0 + l;
     const bool active = rx < nx;
     const int cx = grid_pos(min(rx, nx - 1), W, B, step);
-    const int left = max(cx - R, 0), right = min(cx + R, W - B);
-    const int kmin = max(cy - R, 0) - (cy - R), kmax = min(cy + R, H - B) - (cy - R);
+    // the window's own range Rr <= R: a kernel built for range R serves any
+    // smaller range, its rows and columns beyond Rr masked or skipped
+    const int Rr = mb.range;
+    const int left = max(cx - Rr, 0), right = min(cx + Rr, W - B);
+    const int kmin = max(cy - Rr, 0) - (cy - R), kmax = min(cy + Rr, H - B) - (cy - R);
     const int tc0 = cx - R - X0 + HB * half;  // tile column of this half's first block column at dx = -R
 
     // this half's 8x4 reference block as column pairs (c, c+1) of each row
@@ -149,7 +152,8 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     const float2 neg1 = make_float2(-1.f, -1.f);
     // this part's columns, walked outwards from the window centre so the
     // closest candidates (usually the best) fill the list first
-    const int d0 = part * CPW, d1 = min(NC, d0 + CPW);
+    const int cpw = (2 * Rr + P) / P;  // ceil((2 Rr + 1) / P)
+    const int d0 = (R - Rr) + part * cpw, d1 = min(R + Rr + 1, d0 + cpw);
     const bool down = d1 - 1 <= R;
     for (int m = 0; m < d1 - d0; ++m) {
         const int dxi = down ? d1 - 1 - m : d0 + m;
@@ -321,21 +325,27 @@ bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t s
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8) return false;
     const MatchTune t = tune ? *tune : MatchTune{};
-    // the instantiated ranges; a column's 2R + 1 candidates take one bit each
-    // of a 32- or 64-bit pass mask
-    switch (bm_range) {
-        case 4: return launch_r<4>(mb, group, t, stream);
-        case 5: return launch_r<5>(mb, group, t, stream);
-        case 6: return launch_r<6>(mb, group, t, stream);
-        case 7: return launch_r<7>(mb, group, t, stream);
-        case 8: return launch_r<8>(mb, group, t, stream);
-        case 9: return launch_r<9>(mb, group, t, stream);
-        case 12: return launch_r<12>(mb, group, t, stream);
-        case 15: return launch_r<15>(mb, group, t, stream);
-        case 16: return launch_r<16>(mb, group, t, stream);
-        case 25: return launch_r<25>(mb, group, t, stream);
-        default: return false;
+    // ranges 4-31 (a column's 2R + 1 candidates take one bit each of a 32- or
+    // 64-bit pass mask): the kernel built for the range, or for the next
+    // larger range that has one
+    mb.range = bm_range;
+    if (bm_range < 4) return false;
+    if (bm_range <= 9) {
+        switch (bm_range) {
+            case 4: return launch_r<4>(mb, group, t, stream);
+            case 5: return launch_r<5>(mb, group, t, stream);
+            case 6: return launch_r<6>(mb, group, t, stream);
+            case 7: return launch_r<7>(mb, group, t, stream);
+            case 8: return launch_r<8>(mb, group, t, stream);
+            default: return launch_r<9>(mb, group, t, stream);
+        }
     }
+    if (bm_range <= 12) return launch_r<12>(mb, group, t, stream);
+    if (bm_range <= 15) return launch_r<15>(mb, group, t, stream);
+    if (bm_range <= 16) return launch_r<16>(mb, group, t, stream);
+    if (bm_range <= 25) return launch_r<25>(mb, group, t, stream);
+    if (bm_range <= 31) return launch_r<31>(mb, group, t, stream);
+    return false;
 }
 
 bool launch_match8(const float* plane, int64_t stride, int width, int height, int step, int bm_range, int group,
