@@ -25,6 +25,10 @@ struct MatchPlane {
     int32_t* count;    // njobs
     int W, H, nx, ny;
     int cta0;          // first CTA of this plane in the launch
+    // 8x8 matcher only: int64 words to zero while matching (the plane's
+    // origin weights, cleared for the group filter that follows), or null
+    long long* clear = nullptr;
+    int64_t clear_words = 0;
 };
 struct MatchBatch {
     int n, step;

@@ -118,6 +118,15 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
             cp_async4(dst + swz(c), ok ? src + gx : src, ok ? 4 : 0);
         }
     }
+    // this tile's share of the plane's words to clear, stored while the
+    // window rows are in flight (an even count per tile: 16-byte stores)
+    if (P_.clear) {
+        const int tiles = chunks * P_.ny;
+        const int64_t per = ((P_.clear_words + tiles - 1) / tiles + 1) & ~int64_t(1);
+        const int64_t a = (int64_t)local * per, b = min(P_.clear_words, a + per);
+        for (int64_t i = a + 2 * threadIdx.x; i + 1 < b; i += 2 * (int64_t)blockDim.x)
+            *reinterpret_cast<longlong2*>(P_.clear + i) = make_longlong2(0, 0);
+    }
     cp_async_wait_all();
     __syncthreads();
 

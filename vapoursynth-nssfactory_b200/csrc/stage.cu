@@ -33,20 +33,35 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
     MatchBatch& mb = t.match;
     mb.n = 0;
     mb.step = sp.step;
+    // the 8x8 matcher zeroes the planes' origin weights while it runs when
+    // every plane of the set is matched here (no plane borrowing another's
+    // groups) and the weights allow 16-byte stores
+    bool fuse_clear = true;
+    for (int q = 0; q < ns; ++q) {
+        const StagePlane& it = planes[set[q]];
+        fuse_clear &= !it.shared_pos && (it.acc.pitch * it.h) % 2 == 0 &&
+                      reinterpret_cast<uintptr_t>(it.acc.wsum) % 16 == 0;
+    }
     for (int q = 0; q < ns; ++q) {
         const StagePlane& it = planes[set[q]];
         if (it.shared_pos) continue;
-        mb.p[mb.n++] = MatchPlane{wiener ? it.ref : it.src, wiener ? it.rstride : it.sstride, it.sc->pos, nullptr,
-                                  it.sc->count, it.w, it.h, 0, 0, 0};
+        MatchPlane m{wiener ? it.ref : it.src, wiener ? it.rstride : it.sstride, it.sc->pos, nullptr,
+                     it.sc->count, it.w, it.h, 0, 0, 0};
+        if (fuse_clear) {
+            m.clear = it.acc.wsum;
+            m.clear_words = it.acc.pitch * it.h;
+        }
+        mb.p[mb.n++] = m;
         clock.count_match(it.w, it.h, sp);
     }
+    bool cleared = false;
     if (mb.n > 0) {
         bool ok = false;
         if (sp.block == 8) {
             clock.begin(StageClock::kMatch);
             if (tunes.match.form == 1 && tunes.match.tc)
                 ok = launch_match_tc_batch(mb, sp.bm_range, sp.group, tunes.match.tc, stream);
-            if (!ok) ok = launch_match8_batch(mb, sp.bm_range, sp.group, stream, &tunes.match);
+            if (!ok) cleared = ok = launch_match8_batch(mb, sp.bm_range, sp.group, stream, &tunes.match);
             clock.end(StageClock::kMatch);
         }
         if (!ok) {
@@ -72,11 +87,13 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
                                   it.sp->sigma, it.w, it.h, 0};
         gb.total_jobs += jobs;
     }
-    clock.begin(StageClock::kOther);
-    // about four CTAs per SM over all planes of the set (rows grid-strided)
-    clear_wsum_kernel<<<dim3(std::max(8, std::min(512, ceil_div(592, gb.n))), gb.n), 256, 0, stream>>>(gb);
-    NSSB_CUDA(cudaGetLastError());
-    clock.end(StageClock::kOther);
+    if (!(cleared && fuse_clear)) {
+        clock.begin(StageClock::kOther);
+        // about four CTAs per SM over all planes of the set (rows grid-strided)
+        clear_wsum_kernel<<<dim3(std::max(8, std::min(512, ceil_div(592, gb.n))), gb.n), 256, 0, stream>>>(gb);
+        NSSB_CUDA(cudaGetLastError());
+        clock.end(StageClock::kOther);
+    }
     bool gok = false;
     if (sp.block == 8) {
         clock.begin(StageClock::kGroup);
