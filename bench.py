@@ -340,7 +340,7 @@ def our_arm(args):
                 "d2h_bytes_per_step": nf * PLANE_BYTES},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
-                     "kernel": "spatial_match_kernel (exact FP32 SSD + top-k)",
+                     "kernel": "match8_kernel (exact FP32 SSD + top-k; its tiles also zero the stage's origin weights)",
                      "peak_kind": f"derived: 148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz ({peak_kind} max clock)",
                      "avg_launch_ms": per_launch_ms, "flops_per_launch": flops_per_launch},
         "gpu_launches": int(binfo.kernel_launches) * args.steps,
