@@ -60,7 +60,7 @@ def parse():
                     help="skip the temporal (C3), mixed-batch (C4) and served legs (profiling runs)")
     ap.add_argument("--served-workers", type=int, default=8, help="temporal requests the server runs at once")
     ap.add_argument("--c3-frames", type=int, default=60)
-    ap.add_argument("--only", choices=["c3", "c4", "served"], help="run one leg alone (profiling)")
+    ap.add_argument("--only", choices=["c3", "c4", "served", "refgpu"], help="run one leg alone (profiling)")
     ap.add_argument("--served-plain", type=int, default=300,
                     help="requests of the same stream rendered by the per-frame drop-in for comparison")
     return ap.parse_args()
@@ -226,7 +226,8 @@ def our_arm(args):
         legs = {"c3": lambda: c3_leg(nssb, synth, dev, args.c3_frames, False),
                 "c4": lambda: c4_leg(nssb, synth, dev),
                 "served": lambda: served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
-                                             args.served_workers)}
+                                             args.served_workers),
+                "refgpu": lambda: refgpu_only(nssb, synth, dev, args)}
         print(json.dumps({"leg": args.only, **legs[args.only]()}), flush=True)
         return
     nf = args.frames
@@ -349,6 +350,11 @@ def our_arm(args):
         "clocks": clock,
     }
     if not args.no_legs:
+        out["reference_gpu"] = reference_gpu_leg(nssb, dframes, dout, args.steps, args.warmup)
+        out["reference_gpu"]["ours_batched_over_reference"] = value / out["reference_gpu"]["fps"] \
+            if "fps" in out["reference_gpu"] else None
+        out["reference_gpu"]["ours_plain_over_reference"] = plain_value / out["reference_gpu"]["fps"] \
+            if "fps" in out["reference_gpu"] else None
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
         out["batched_c4"] = c4_leg(nssb, synth, dev)
     # the headline's batch layouts and nodes are released before the served
@@ -370,6 +376,7 @@ def our_arm(args):
         import oracle as O
 
         threads = O.host_threads()
+        out["c2_parity"] = c2_parity_leg(frames, dout, threads)
         fps, done, el = cpu_leg(frames, threads)
         out["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                                "sample": f"{done} of the workload's frames, frame-parallel, {el:.1f} s; CPU "
@@ -378,6 +385,119 @@ def our_arm(args):
         print(json.dumps(out), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def reference_gpu_leg(nssb, dframes, ours, steps, warmup, heavy_frames=4):
+    """The reference's own CUDA kernels (oracle/_ref/libref_bm3d_gpu.so: its
+    bm3d/kernels.cu and common/match*.cu / aggregate.cu compiled unchanged for
+    sm_100a, driven the way its per-frame driver does) on the same
+    device-resident frames, on the stream the events record on: every plane
+    of every frame, hard-threshold stage then Wiener stage. Also the output
+    agreement with this build's frames (`ours`) and the reference's "heavy"
+    preset (final=1, block_step=3, group_size=32, group_size_basic=16,
+    bm_range=19) on both sides."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import refgpu as R
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref/libref_bm3d_gpu.so not built (needs the reference sources)"}
+    sig = O.effective_sigma(SIGMA)
+    ctx = R.RefGpu()
+    basic = {p.shape: torch.empty_like(p) for p in dframes[0]}
+    outs = [tuple(torch.empty_like(p) for p in f) for f in dframes]
+
+    def render(frames, dst, shape=(8, 8, 8, 9, 8)):
+        block, step, group_b, rng_, group_f = shape
+        for f, o in zip(frames, dst):
+            for p, q in zip(f, o):
+                h, w = p.shape
+                b = basic[p.shape]
+                ctx.stage(p.data_ptr(), None, b.data_ptr(), w, h, sig, block, step, rng_, group_b)
+                ctx.stage(p.data_ptr(), b.data_ptr(), q.data_ptr(), w, h, sig, block, step, rng_, group_f)
+
+    for _ in range(warmup):
+        render(dframes, outs)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        render(dframes, outs)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    fps = len(dframes) * steps / (ms / 1e3)
+    psnrs = [O.psnr([a.cpu().numpy() for a in fo], [b.cpu().numpy() for b in fr]) for fo, fr in zip(ours, outs)]
+    res = {"fps": fps, "ms_per_step": ms / steps,
+           "psnr_ours_vs_reference_kernels_db_min": float(min(psnrs)),
+           "psnr_frames": len(psnrs),
+           "matcher": R.matcher_kind(W, H, 8, 8, 9, 8),
+           "what": "the reference's src/cuda kernels compiled unchanged for sm_100a; per plane: fixed_clear, "
+                   "spatial_match, bm3d_filter_groups, fixed_finish, for each stage, on one stream"}
+    # the heavy preset, a few frames
+    hf = dframes[:heavy_frames]
+    ho = outs[:heavy_frames]
+    heavy = (8, 3, 16, 19, 32)
+    render(hf, ho, heavy)
+    torch.cuda.synchronize()
+    s.record()
+    render(hf, ho, heavy)
+    e.record()
+    torch.cuda.synchronize()
+    res["heavy_fps"] = len(hf) / (s.elapsed_time(e) / 1e3)
+    node = nssb.BM3D(nssb.Clip.from_frames(hf, nssb.YUV, 1, 1), sigma=SIGMA, final=1, block_step=3, group_size=32,
+                     group_size_basic=16, bm_range=19)
+    mine = [tuple(torch.empty_like(p) for p in f) for f in hf]
+    for n in range(len(hf)):
+        node.get_frame(n, out=mine[n])
+    torch.cuda.synchronize()
+    s.record()
+    for n in range(len(hf)):
+        node.get_frame(n, out=mine[n])
+    e.record()
+    torch.cuda.synchronize()
+    node.close()
+    res["heavy_ours_plain_fps"] = len(hf) / (s.elapsed_time(e) / 1e3)
+    res["heavy_psnr_ours_vs_reference_kernels_db_min"] = float(min(
+        O.psnr([a.cpu().numpy() for a in fo], [b.cpu().numpy() for b in fr]) for fo, fr in zip(mine, ho)))
+    res["heavy_matchers"] = {"basic": R.matcher_kind(W, H, 8, 3, 19, 16), "final": R.matcher_kind(W, H, 8, 3, 19, 32)}
+    res["heavy_workload"] = (f"{len(hf)} of the frames, final=1, block_step=3, group_size=32, group_size_basic=16, "
+                             "bm_range=19 (the reference's published 'heavy' preset: 29 fps on an RTX 5080)")
+    ctx.close()
+    return res
+
+
+def refgpu_only(nssb, synth, dev, args):
+    """The reference-kernel leg alone on the headline frames (profiling runs)."""
+    import torch
+
+    frames = synth.yuv420_clip(1000, W, H, args.frames, SIGMA)
+    dframes = [tuple(torch.from_numpy(p).to(dev) for p in f) for f in frames]
+    node = nssb.BM3D(nssb.Clip.from_frames(dframes, nssb.YUV, 1, 1), sigma=SIGMA, final=1)
+    ours = [tuple(torch.empty_like(p) for p in f) for f in dframes]
+    for n in range(len(dframes)):
+        node.get_frame(n, out=ours[n])
+    node.close()
+    return reference_gpu_leg(nssb, dframes, ours, args.steps, args.warmup)
+
+
+def c2_parity_leg(frames, gpu_out, threads, n=16):
+    """Full-size parity of the headline: this build's output frames against
+    the CPU restatement on the first n frames (1920x1080 YUV420, two-stage)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    st = O.stage(O.effective_sigma(SIGMA))
+    k = min(n, len(frames))
+    t0 = time.perf_counter()
+    lum = O.frames_mt([f[0] for f in frames[:k]], st, st, threads)
+    chroma = O.frames_mt([p for f in frames[:k] for p in f[1:]], st, st, threads)
+    ps = [O.psnr([lum[i], chroma[2 * i], chroma[2 * i + 1]], [p.cpu().numpy() for p in gpu_out[i]]) for i in range(k)]
+    return {"frames": k, "psnr_vs_cpu_db_min": float(min(ps)), "psnr_vs_cpu_db_mean": float(np.mean(ps)),
+            "cpu_s": time.perf_counter() - t0, "note": "full 1920x1080 YUV420 frames, batched form vs the CPU "
+            "restatement (oracle/), PSNR pooled over the three planes per frame"}
 
 
 def accuracy_leg(nssb, frame, dev):

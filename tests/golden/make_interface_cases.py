@@ -7,11 +7,14 @@ keyword arguments of the call (decoded from the case key the way that test
 builds it) and the expected outcome (output format/size or the exact error).
 Run in a tree that has the reference checked out:
 
-    python tests/golden/make_interface_cases.py --reference /root/reference
+    python tests/golden/make_interface_cases.py --reference <reference checkout>
+
+(or with the checkout's path in the NSS_REFERENCE environment variable).
 """
 import argparse
 import ast
 import json
+import os
 from pathlib import Path
 
 INT_PROBES = (-1, 0, 1, 2, 3, 4, 7, 8, 9, 16, 17, 33, 65, 1000)
@@ -54,8 +57,10 @@ def decode(spec: str) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NSS_REFERENCE"))
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference checkout with --reference or NSS_REFERENCE")
     golden = json.loads((Path(args.reference) / "tests/data/plugin_interface_v1.json").read_text())
     cases = []
     for key in sorted(golden["cases"]):

@@ -25,9 +25,19 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
 
 // Fixed-point scale of the aggregation sums: num and the per-origin weights
 // are int64 multiples of 2^-32, so the sums do not depend on the order in
-// which groups land (deterministic in any launch shape or batch mix).
-constexpr double kFixedScale = 4294967296.0;
-constexpr double kFixedInv = 1.0 / 4294967296.0;
+// which groups land (deterministic in any launch shape or batch mix). All of
+// it is FP32 and integer arithmetic: a sample w * v is rounded once in FP32,
+// scaled by 2^32 (exact: a power of two) and rounded to the nearest integer.
+constexpr float kFixedScale = 4294967296.f;
+constexpr float kFixedInv = 1.f / 4294967296.f;
+
+#ifdef __CUDACC__
+__device__ __forceinline__ long long to_fixed(float x) { return __float2ll_rn(x * kFixedScale); }
+// num / den of two fixed-point sums (the common 2^-32 cancels)
+__device__ __forceinline__ float fixed_quotient(long long num, long long den) {
+    return __fdiv_rn(__ll2float_rn(num), __ll2float_rn(den));
+}
+#endif
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int grid_count(int extent, int block, int step) {

@@ -48,14 +48,8 @@ __global__ void __launch_bounds__(kTX* kTY) finish_kernel(const long long* __res
     const int x = x0 + c, y = y0 + r;
     if (x >= W || y >= H) return;
     const long long d = den[r][c];
-    const double dd = (double)d * kFixedInv;
-    float out;
-    if ((float)dd > 1e-12f) {
-        out = (float)((double)num[(int64_t)y * as + x] / (double)d);
-    } else {
-        out = src[(int64_t)y * ss + x];
-    }
-    dst[(int64_t)y * ds + x] = out;
+    // den > 1e-12 in real units is d >= 1 in units of 2^-32
+    dst[(int64_t)y * ds + x] = d > 0 ? fixed_quotient(num[(int64_t)y * as + x], d) : src[(int64_t)y * ss + x];
 }
 
 __global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restrict__ num,
@@ -70,8 +64,8 @@ __global__ void __launch_bounds__(kTX* kTY) fat_kernel(const long long* __restri
     const int r = threadIdx.x / kTX, c = threadIdx.x % kTX;
     const int x = x0 + c, y = y0 + r;
     if (x >= W || y >= H) return;
-    dnum[(int64_t)y * ds + x] = (float)((double)num[(int64_t)y * as + x] * kFixedInv);
-    dden[(int64_t)y * ds + x] = (float)((double)den[r][c] * kFixedInv);
+    dnum[(int64_t)y * ds + x] = __ll2float_rn(num[(int64_t)y * as + x]) * kFixedInv;
+    dden[(int64_t)y * ds + x] = __ll2float_rn(den[r][c]) * kFixedInv;
 }
 
 // Batched finish over a plane table. A CTA finishes a 64 x 32 tile:
@@ -200,7 +194,7 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
         if (j > 0) den += row[vs_col(8 * seg + j + B - 1)] - row[vs_col(8 * seg + j - 1)];
         // den > 1e-12 in real units is den >= 1 in units of 2^-32 (the
         // smallest positive den, 2^-32 = 2.3e-10, already passes)
-        out[j] = den > 0 ? (float)((double)nv[j] / (double)den) : sv[j];
+        out[j] = den > 0 ? fixed_quotient(nv[j], den) : sv[j];
     }
     if (vec) {
 #pragma unroll

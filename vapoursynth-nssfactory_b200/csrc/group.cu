@@ -35,7 +35,12 @@ __host__ __device__ constexpr int dct_offset(int n) {
 
 std::once_flag g_tables_once[64];
 
-void ensure_tables() {
+}  // namespace
+
+// Uploads the DCT tables to the current device once (a synchronous copy: the
+// first call on a device must not be made under stream capture). An upload
+// that throws leaves the flag unset, so the next call tries again.
+void ensure_group_tables() {
     int dev = 0;
     NSSB_CUDA(cudaGetDevice(&dev));
     std::call_once(g_tables_once[dev & 63], [] {
@@ -50,6 +55,8 @@ void ensure_tables() {
         NSSB_CUDA(cudaMemcpyToSymbol(g_dct_tables, host, sizeof host));
     });
 }
+
+namespace {
 
 __device__ __forceinline__ float haar_scale(int n, int j) {
     int e = 0;
@@ -116,10 +123,6 @@ __device__ void dct2(float* cube, int G, const float* T, bool inverse, int cubes
         dct_line<B>(cube + c * cube_stride + g * A + j, B, T, inverse);
     }
     __syncthreads();
-}
-
-__device__ __forceinline__ long long to_fixed(float w, float v) {
-    return __double2ll_rn((double)w * (double)v * kFixedScale);
 }
 
 template <int B>
@@ -220,14 +223,14 @@ __global__ void __launch_bounds__(128) group_kernel(GroupIO io, int W, int H, co
             const int s = js ? js[g] : 0;
             const int64_t off = (int64_t)(pos_y(p) + i) * io.acc_stride + pos_x(p) + j;
             atomicAdd(reinterpret_cast<unsigned long long*>(io.num[s] + off),
-                      static_cast<unsigned long long>(to_fixed(weight, cube[idx])));
+                      static_cast<unsigned long long>(to_fixed(__fmul_rn(weight, cube[idx]))));
         }
         for (int g = tid; g < k; g += blockDim.x) {
             const int32_t p = jp[g];
             const int s = js ? js[g] : 0;
             const int64_t off = (int64_t)pos_y(p) * io.acc_stride + pos_x(p);
             atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[s] + off),
-                      static_cast<unsigned long long>(__double2ll_rn((double)weight * kFixedScale)));
+                      static_cast<unsigned long long>(to_fixed(weight)));
         }
         __syncthreads();
     }
@@ -270,7 +273,7 @@ void launch_group_filter(const GroupIO& io, int width, int height, const int32_t
                          float* scratch, size_t scratch_floats, cudaStream_t stream) {
     if (njobs <= 0) return;
     if (block == 8 && launch_group8(io, pos, slot, count, njobs, group, sigma, wiener, stream)) return;
-    ensure_tables();
+    ensure_group_tables();
     switch (block) {
         case 1: return launch_group_b<1>(io, width, height, pos, slot, count, njobs, group, sigma, wiener, scratch, scratch_floats, stream);
         case 2: return launch_group_b<2>(io, width, height, pos, slot, count, njobs, group, sigma, wiener, scratch, scratch_floats, stream);

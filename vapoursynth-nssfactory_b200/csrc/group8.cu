@@ -245,9 +245,9 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
         weight = __fdiv_rn(1.f, (float)(kept > 1 ? kept : 1));
     }
-    // weight x value x 2^32 is exact in double (a 24 x 24-bit product and a
-    // power of two), so scaling the weight first rounds the same
-    const double wscaled = (double)weight * kFixedScale;
+    // w * v rounds once in FP32; the 2^32 scale is exact, so it goes on the
+    // weight first: (w 2^32) v == (w v) 2^32 bit for bit (barring overflow)
+    const float wscaled = weight * kFixedScale;
     __syncwarp();
     if constexpr (G <= 8) {
         // inverse rows in the cube, then inverse columns kept in registers and
@@ -265,7 +265,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         }
         __syncwarp();
         if (g < k) {
-            if (q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
+            if (q == 0) add_weight(s, px, py, __float2ll_rn(wscaled));
 #pragma unroll
             for (int t = 0; t < Sh::RPL; ++t) {
                 const int c = q + Sh::LP * t;
@@ -274,7 +274,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
                 for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + Sh::at(i, c)];
                 idct8(v);
 #pragma unroll
-                for (int i = 0; i < 8; ++i) add_num(s, px + c, py + i, __double2ll_rn(wscaled * (double)v[i]));
+                for (int i = 0; i < 8; ++i) add_num(s, px + c, py + i, __float2ll_rn(__fmul_rn(wscaled, v[i])));
             }
         }
     } else {
@@ -294,7 +294,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 #pragma unroll
             for (int j = 0; j < 8; ++j) cube[g * Sh::S + Sh::at(row, j)] = v[j];
         }
-        if (g < k && q == 0) add_weight(s, px, py, __double2ll_rn(wscaled));
+        if (g < k && q == 0) add_weight(s, px, py, __float2ll_rn(wscaled));
         __syncwarp();
 #pragma unroll
         for (int gg = 0; gg < G; ++gg) {
@@ -305,7 +305,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
             for (int h = 0; h < 2; ++h) {
                 const int i = 4 * h + (lane >> 3), j = lane & 7;
                 add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
-                        __double2ll_rn(wscaled * (double)cube[gg * Sh::S + Sh::at(i, j)]));
+                        __float2ll_rn(__fmul_rn(wscaled, cube[gg * Sh::S + Sh::at(i, j)])));
             }
         }
     }

@@ -171,6 +171,8 @@ struct GroupSlotBatch {
 bool launch_group8_slots_batch(const GroupSlotBatch& batch, int group, bool wiener, cudaStream_t stream);
 // Device scratch (floats) the generic group kernel needs for this shape, 0 if none.
 size_t group_filter_scratch_floats(int block, int group, bool wiener);
+// The generic group kernel's DCT tables on the current device (once per device).
+void ensure_group_tables();
 
 // out = den > 1e-12 ? num / den : src, den the B x B box sum of the origin
 // weights; num and wsum are read, not cleared.

@@ -13,8 +13,10 @@
 // the process exits. The array's name in host code is only a host-side
 // stand-in, never a device address: its device address is looked up once per
 // device with cudaGetSymbolAddress (with that device current) on the first
-// call on that device, and passed to the kernels. Make that first call
-// before any stream capture.
+// call on that device, and passed to the kernels; the same set-up uploads the
+// generic group kernel's DCT tables to the device. Make that first call
+// before any stream capture. A set-up that fails (under capture, say) is not
+// remembered: the next call on that device tries again.
 //
 // All calls share the array and it keeps the last call's contents: each call
 // clears the sums it accumulates into before use. Calls that overlap on the
@@ -43,21 +45,21 @@ static_assert(kNumBytes % 256 == 0 && kWsumBytes % 256 == 0 && kPosBytes % 256 =
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kMaxDevices = 64;
-std::once_flag g_setup_once[kMaxDevices];
-unsigned char* g_scratch_ptr[kMaxDevices];
-cudaError_t g_setup_error[kMaxDevices];
+std::mutex g_setup_mutex;
+unsigned char* g_scratch_ptr[kMaxDevices];  // set only once a set-up succeeded
 
 unsigned char* scratch_for_current_device() {
     int dev = 0;
     NSSB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw std::invalid_argument("nss_cuda: device index beyond the no-allocation table");
-    std::call_once(g_setup_once[dev], [dev] {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_ptr[dev]) {
+        ensure_group_tables();
         void* p = nullptr;
-        g_setup_error[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        NSSB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        if (!p) throw CudaError("nss_cuda: cudaGetSymbolAddress gave no address for the stage scratch");
         g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
-    });
-    NSSB_CUDA(g_setup_error[dev]);
-    if (!g_scratch_ptr[dev]) throw CudaError("nss_cuda: cudaGetSymbolAddress gave no address for the stage scratch");
+    }
     return g_scratch_ptr[dev];
 }
 
