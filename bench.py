@@ -356,7 +356,7 @@ def our_arm(args):
         out["reference_gpu"]["ours_plain_over_reference"] = plain_value / out["reference_gpu"]["fps"] \
             if "fps" in out["reference_gpu"] else None
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
-        out["batched_c4"] = c4_leg(nssb, synth, dev)
+        out["batched_c4"] = c4_leg(nssb, synth, dev, check_psnr=rank == 0 and world == 1 and not args.no_cpu)
     # the headline's batch layouts and nodes are released before the served
     # leg sizes its memory budget from the device's free memory
     batch.close()
@@ -483,6 +483,28 @@ def refgpu_only(nssb, synth, dev, args):
     return reference_gpu_leg(nssb, dframes, ours, args.steps, args.warmup)
 
 
+def cpu_two_stage(frames, sigma, radius, threads):
+    """The CPU restatement's two-stage output of a clip (list of plane tuples),
+    plane by plane on a thread pool (the oracle's C calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    st = O.stage(O.effective_sigma(sigma))
+
+    def plane(i):
+        ps = [f[i] for f in frames]
+        if radius == 0:
+            return [O.bm3d_plane_two_stage(p, st, st)[0] for p in ps]
+        basic = O.bm3d_clip_plane(ps, st, radius)
+        return O.bm3d_clip_plane(ps, st, radius, ref_frames=basic)
+
+    with ThreadPoolExecutor(max(1, min(threads, len(frames[0])))) as ex:
+        per_plane = list(ex.map(plane, range(len(frames[0]))))
+    return [tuple(per_plane[i][n] for i in range(len(frames[0]))) for n in range(len(frames))]
+
+
 def c2_parity_leg(frames, gpu_out, threads, n=16):
     """Full-size parity of the headline: this build's output frames against
     the CPU restatement on the first n frames (1920x1080 YUV420, two-stage)."""
@@ -579,24 +601,27 @@ def c3_leg(nssb, synth, dev, frames_n, check_psnr):
     res["precision_equals_fp32_bitwise"] = bool(same)
     res["group_index_agreement"] = 1.0 if same else None
     if check_psnr:
-        # the CPU restatement on a 256x144 crop of the first 5 frames' luma (the oracle is slow at 1080p)
+        # full 1920x1080 YUV420 frames: the first 5 frames as a 5-frame clip,
+        # the precision form against the CPU restatement
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
 
-        crop = [np.ascontiguousarray(f[0][200:344, 400:656]) for f in frames[:5]]
-        node = nssb.BM3D(nssb.Clip.from_frames([(c,) for c in crop], nssb.GRAY), sigma=10.0, radius=2, final=1)
+        t0 = time.perf_counter()
+        k = min(5, frames_n)
+        node = nssb.BM3D(nssb.Clip.from_frames(d[:k], nssb.YUV, 1, 1), sigma=10.0, radius=2, final=1)
         node.set_matcher(1)
-        got = [node.get_frame(n)[0] for n in range(5)]
+        got = [[p.cpu().numpy() for p in node.get_frame(n)] for n in range(k)]
         node.close()
-        st = O.stage(O.effective_sigma(10.0))
-        basic = O.bm3d_clip_plane(crop, st, 2)
-        want = O.bm3d_clip_plane(crop, st, 2, ref_frames=basic)
-        res["psnr_vs_cpu_db_min"] = float(min(O.psnr(g, w) for g, w in zip(got, want)))
-        res["psnr_sample"] = "256x144 luma crop of the first 5 frames, precision form vs the CPU restatement"
+        want = cpu_two_stage(frames[:k], 10.0, 2, O.host_threads())
+        ps = [O.psnr(g, w) for g, w in zip(got, want)]
+        res["psnr_vs_cpu_db_min"] = float(min(ps))
+        res["psnr_vs_cpu_db_mean"] = float(np.mean(ps))
+        res["psnr_sample"] = (f"{k} full 1920x1080 YUV420 frames (a {k}-frame clip of the sequence), precision form "
+                              f"vs the CPU restatement; {time.perf_counter() - t0:.1f} s")
     return res
 
 
-def c4_leg(nssb, synth, dev, seed=4000):
+def c4_leg(nssb, synth, dev, seed=4000, check_psnr=False):
     """64 frames of uneven sizes (16 x 854x480, 16 x 1280x720, 24 x 1920x1080,
     8 x 3840x2160), each Gray or YUV420PS (seeded choice), sigma drawn from
     {3, 5, 10, 20}, two-stage, radius 0: the per-frame drop-in vs one batched
@@ -605,7 +630,7 @@ def c4_leg(nssb, synth, dev, seed=4000):
 
     rng = np.random.default_rng(seed)
     sizes = [(854, 480)] * 16 + [(1280, 720)] * 16 + [(1920, 1080)] * 24 + [(3840, 2160)] * 8
-    nodes, reqs, outs = [], [], []
+    nodes, reqs, outs, host, sigmas = [], [], [], [], []
     kinds = {"gray": 0, "yuv420": 0}
     for i, (w, h) in enumerate(sizes):
         sigma = float(rng.choice([3.0, 5.0, 10.0, 20.0]))
@@ -617,6 +642,8 @@ def c4_leg(nssb, synth, dev, seed=4000):
             f = (synth.gray_frame(seed + i, w, h, sigma)[0],)
             clip = nssb.Clip.from_frames([tuple(torch.from_numpy(p).to(dev) for p in f)], nssb.GRAY)
         kinds["yuv420" if yuv else "gray"] += 1
+        host.append(f)
+        sigmas.append(sigma)
         node = nssb.BM3D(clip, sigma=sigma, final=1)
         nodes.append(node)
         reqs.append((node, 0))
@@ -655,6 +682,23 @@ def c4_leg(nssb, synth, dev, seed=4000):
                             "match_persistent": inf.match_persistent, "group_warps": inf.group_warps,
                             "group_ctas_per_sm": inf.group_ctas_per_sm, "kernels_per_step": int(inf.kernel_launches),
                             "graph": bool(inf.graphs)}
+    if check_psnr:
+        # one frame of each resolution (the first of each) against the CPU restatement
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        t0 = time.perf_counter()
+        firsts = [sizes.index(s) for s in ((854, 480), (1280, 720), (1920, 1080), (3840, 2160))]
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(len(firsts)) as ex:
+            wants = list(ex.map(lambda i: cpu_two_stage([host[i]], sigmas[i], 0, O.host_threads())[0], firsts))
+        ps = {f"{sizes[i][0]}x{sizes[i][1]}": O.psnr([p.cpu().numpy() for p in outs[i]], w)
+              for i, w in zip(firsts, wants)}
+        res["psnr_vs_cpu_db"] = ps
+        res["psnr_vs_cpu_db_min"] = float(min(ps.values()))
+        res["psnr_sample"] = (f"the first frame of each resolution (batched form) vs the CPU restatement; "
+                              f"{time.perf_counter() - t0:.1f} s")
     batch.close()
     for node in nodes:
         node.close()
@@ -747,6 +791,18 @@ def served_leg(nssb, synth, local, n_req, n_plain, workers=8):
             same &= all(np.array_equal(a, b) for a, b in zip(node.get_frame(n), check_out[i][n]))
         node.close()
     served["served_equals_plain_bitwise"] = bool(same)
+    # and against the CPU restatement
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    ps = []
+    for i in check_ids:
+        rq = reqs[i]
+        want = cpu_two_stage(pool["480p"][:rq["frames"]], rq["sigma"], rq["radius"], O.host_threads())
+        ps.append(O.psnr([p for f in check_out[i] for p in f], [p for f in want for p in f]))
+    served["psnr_vs_cpu_db_min"] = float(min(ps)) if ps else None
+    served["psnr_sample"] = (f"{len(check_ids)} served 480p requests (radius "
+                             f"{sorted(set(reqs[i]['radius'] for i in check_ids))}) vs the CPU restatement")
     # the per-frame drop-in, first come first served, on the first n_plain requests
     plat, pdone = [], []
     t0 = time.perf_counter()

@@ -132,9 +132,11 @@ int nssb_bm3d_create(const nssb_video_info* clip, const nssb_video_info* ref, co
         // changes the output
         if (cfg.memory_limit_mb > 0) {
             const size_t need = nssb::Engine::footprint(cfg, true);
+            const int streams = cfg.radius > 0 ? 1 : std::max(1, cfg.num_streams);
             if (need > (size_t)cfg.memory_limit_mb << 20)
-                throw nssb::ArgumentError("nss_cuda.BM3D: memory_limit_mb is too small for this clip: each of the 1 "
-                                          "stream(s) needs at least " + std::to_string((need >> 20) + 1) + " MiB");
+                throw nssb::ArgumentError("nss_cuda.BM3D: memory_limit_mb is too small for this clip: each of the " +
+                                          std::to_string(streams) + " stream(s) needs at least " +
+                                          std::to_string((need / streams >> 20) + 1) + " MiB");
         }
         h->engine = std::make_unique<nssb::Engine>(cfg);
         *out = h.release();

@@ -79,11 +79,16 @@ int64_t pitch_of(int w) { return (int64_t)((w + 31) / 32) * 32; }
 
 }  // namespace
 
-Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg), tables_(new StageTables) {
+Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg) {
     device_ = cfg.device_id;
     NSSB_CUDA(cudaSetDevice(device_));
-    NSSB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    // radius 0: num_streams slots; temporal: one (its rolling state is sequential)
+    const int n = cfg_.radius > 0 ? 1 : std::max(1, cfg_.num_streams);
+    for (int i = 0; i < n; ++i) slots_.emplace_back(new Slot());
     try {
+        for (auto& s : slots_) NSSB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        stream_ = slots_[0]->stream;
+        clock_.reset(new Clock(this, slots_[0].get()));
         alloc();
     } catch (...) {
         release();
@@ -92,21 +97,51 @@ Engine::Engine(const Bm3dConfig& cfg) : cfg_(cfg), tables_(new StageTables) {
 }
 
 void Engine::release() {
-    if (stream_) (void)cudaStreamSynchronize(stream_);  // nothing queued may still use the buffers
-    for (auto& e : event_pool_) {
-        (void)cudaEventDestroy(e.first);
-        (void)cudaEventDestroy(e.second);
+    for (auto& s : slots_) {
+        if (!s->stream) continue;
+        (void)cudaStreamSynchronize(s->stream);  // nothing queued may still use the buffers
+        for (auto& e : s->events) {
+            (void)cudaEventDestroy(e.first);
+            (void)cudaEventDestroy(e.second);
+        }
+        s->events.clear();
     }
-    event_pool_.clear();
     for (void* p : allocations_) dev_free(p);
     allocations_.clear();
-    if (stream_) {
-        (void)cudaStreamDestroy(stream_);
-        stream_ = nullptr;
+    for (auto& s : slots_) {
+        if (s->stream) (void)cudaStreamDestroy(s->stream);
+        s->stream = nullptr;
+    }
+    stream_ = nullptr;
+}
+
+Engine::Slot* Engine::lease(bool primary) {
+    std::unique_lock<std::mutex> lock(slot_mu_);
+    for (;;) {
+        for (size_t i = 0; i < slots_.size(); ++i) {
+            Slot* s = slots_[i].get();
+            if (!s->busy && (!primary || i == 0)) {
+                s->busy = true;
+                return s;
+            }
+        }
+        slot_cv_.wait(lock);
     }
 }
 
+void Engine::give_back(Slot* s) {
+    {
+        std::lock_guard<std::mutex> lock(slot_mu_);
+        s->busy = false;
+    }
+    slot_cv_.notify_all();
+}
+
 void Engine::alloc() {
+    for (auto& s : slots_) alloc_slot(*s);
+}
+
+void Engine::alloc_slot(Slot& s) {
     auto take = [&](size_t bytes) {
         void* p = dev_alloc(bytes);
         allocations_.push_back(p);
@@ -115,24 +150,24 @@ void Engine::alloc() {
     for (int p = 0; p < cfg_.planes; ++p) {
         const int w = cfg_.plane_w[p], h = cfg_.plane_h[p];
         const int64_t pitch = pitch_of(w);
-        for (DevPlane* d : {&in_[p], &refin_[p], &basic_[p], &out_[p]}) {
+        for (DevPlane* d : {&s.in[p], &s.refin[p], &s.basic[p], &s.out[p]}) {
             d->p = static_cast<float*>(take((size_t)pitch * h * sizeof(float)));
             d->pitch = pitch;
             d->w = w;
             d->h = h;
         }
         // num stays zero between stages: every finish clears what it consumed
-        acc_[p].pitch = pitch;
-        acc_[p].num = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
-        acc_[p].wsum = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
-        NSSB_CUDA(cudaMemsetAsync(acc_[p].num, 0, (size_t)pitch * h * sizeof(long long), stream_));
+        s.acc[p].pitch = pitch;
+        s.acc[p].num = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
+        s.acc[p].wsum = static_cast<long long*>(take((size_t)pitch * h * sizeof(long long)));
+        NSSB_CUDA(cudaMemsetAsync(s.acc[p].num, 0, (size_t)pitch * h * sizeof(long long), s.stream));
         size_t jobs = 0, group = 0, cube = 0;
         for (const StageParams* sp : {&cfg_.final_stage[p], &cfg_.basic_stage[p]}) {
             jobs = std::max(jobs, (size_t)grid_count(w, sp->block, sp->step) * grid_count(h, sp->block, sp->step));
             group = std::max(group, (size_t)sp->group);
             cube = std::max(cube, group_filter_scratch_floats(sp->block, sp->group, true));
         }
-        StageScratch& sc = scratch_[p];
+        StageScratch& sc = s.scratch[p];
         sc.jobs_cap = jobs;
         sc.group_cap = group;
         sc.pos = static_cast<int32_t*>(take(jobs * group * sizeof(int32_t)));
@@ -153,78 +188,96 @@ void Engine::frame_window(int n, int* first, int* last) const {
     *last = std::min(cfg_.vi.num_frames - 1, n + reach);
 }
 
-const float* Engine::device_input(int plane, const nssb_frame* frames, int first, int n, int memory, bool is_ref,
-                                  int64_t* stride) {
+const float* Engine::device_input(Slot& s, int plane, const nssb_frame* frames, int first, int n, int memory,
+                                  bool is_ref, int64_t* stride) {
     const nssb_frame& f = frames[n - first];
     if (memory == NSSB_MEM_DEVICE) {
         *stride = f.strides[plane];
         return f.planes[plane];
     }
-    DevPlane& d = is_ref ? refin_[plane] : in_[plane];
+    DevPlane& d = is_ref ? s.refin[plane] : s.in[plane];
     NSSB_CUDA(cudaMemcpy2DAsync(d.p, d.pitch * sizeof(float), f.planes[plane], f.strides[plane] * sizeof(float),
-                                d.w * sizeof(float), d.h, cudaMemcpyHostToDevice, stream_));
+                                d.w * sizeof(float), d.h, cudaMemcpyHostToDevice, s.stream));
     *stride = d.pitch;
     return d.p;
 }
 
-void Engine::clock_begin(Kind) {
-    if (!timing_) return;
-    const size_t i = pending_.size();
-    if (i >= event_pool_.size()) {
+void Engine::clock_begin(Slot& s, Kind) {
+    bool timing;
+    {
+        std::lock_guard<std::mutex> lock(stats_mu_);
+        timing = timing_;
+    }
+    if (!timing) return;
+    const size_t i = s.pending.size();
+    if (i >= s.events.size()) {
         cudaEvent_t a, b;
         NSSB_CUDA(cudaEventCreate(&a));
         NSSB_CUDA(cudaEventCreate(&b));
-        event_pool_.emplace_back(a, b);
+        s.events.emplace_back(a, b);
     }
-    NSSB_CUDA(cudaEventRecord(event_pool_[i].first, stream_));
+    NSSB_CUDA(cudaEventRecord(s.events[i].first, s.stream));
+    s.pending.emplace_back(-1, i);  // open until clock_end names its kind
 }
 
-void Engine::clock_end(Kind kind) {
-    if (timing_) {
-        const size_t i = pending_.size();
-        NSSB_CUDA(cudaEventRecord(event_pool_[i].second, stream_));
-        pending_.emplace_back((int)kind, i);
+void Engine::clock_end(Slot& s, Kind kind) {
+    if (!s.pending.empty() && s.pending.back().first < 0) {
+        NSSB_CUDA(cudaEventRecord(s.events[s.pending.back().second].second, s.stream));
+        s.pending.back().first = (int)kind;
     }
+    std::lock_guard<std::mutex> lock(stats_mu_);
     ++stats_.launches;
     if (kind == kMatch) ++stats_.match_launches;
     if (kind == kGroup) ++stats_.group_launches;
     if (kind == kFinish) ++stats_.finish_launches;
 }
 
-// After the stream is synchronised: add the bracketed durations.
-void Engine::collect_timing() {
-    for (const auto& p : pending_) {
+// After the slot's stream is synchronised: add the bracketed durations.
+void Engine::collect_timing(Slot& s) {
+    double ms_by_kind[3] = {0, 0, 0};
+    for (const auto& p : s.pending) {
+        if (p.first < 0 || p.first > 2) continue;
         float ms = 0.f;
-        NSSB_CUDA(cudaEventElapsedTime(&ms, event_pool_[p.second].first, event_pool_[p.second].second));
-        if (p.first == kMatch) stats_.match_ms += ms;
-        if (p.first == kGroup) stats_.group_ms += ms;
-        if (p.first == kFinish) stats_.finish_ms += ms;
+        NSSB_CUDA(cudaEventElapsedTime(&ms, s.events[p.second].first, s.events[p.second].second));
+        ms_by_kind[p.first] += ms;
     }
-    pending_.clear();
+    s.pending.clear();
+    std::lock_guard<std::mutex> lock(stats_mu_);
+    stats_.match_ms += ms_by_kind[kMatch];
+    stats_.group_ms += ms_by_kind[kGroup];
+    stats_.finish_ms += ms_by_kind[kFinish];
 }
 
 // Algorithmic work of one matching launch: every reference against every
 // other position of its clamped window, 3 * B^2 flops per pair.
 void Engine::count_match(int w, int h, const StageParams& sp) {
     const double pairs = match_pairs(w, h, sp);
+    std::lock_guard<std::mutex> lock(stats_mu_);
     stats_.match_pairs += pairs;
     stats_.match_flops += pairs * 3.0 * sp.block * sp.block;
 }
 
 void Engine::set_matcher(int form) {
     std::lock_guard<std::mutex> lock(mu_);
+    // every slot idle: no frame may be reading the tunes
+    std::vector<Slot*> held;
+    for (size_t i = 0; i < slots_.size(); ++i) held.push_back(lease(false));
     if (form == 1 && !tunes_.match.tc) {
         auto* c = static_cast<TcCounters*>(dev_alloc(sizeof(TcCounters)));
         allocations_.push_back(c);
         NSSB_CUDA(cudaMemsetAsync(c, 0, sizeof(TcCounters), stream_));
+        NSSB_CUDA(cudaStreamSynchronize(stream_));
         tunes_.match.tc = c;
     }
     tunes_.match.form = form;
+    for (Slot* s : held) give_back(s);
 }
 
 void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
-    std::lock_guard<std::mutex> lock(mu_);
+    std::lock_guard<std::mutex> lock(stats_mu_);
     if (tunes_.match.tc) {
+        // every slot's precision-form kernels add to the counters
+        for (auto& s : slots_) NSSB_CUDA(cudaStreamSynchronize(s->stream));
         TcCounters c{};
         NSSB_CUDA(cudaMemcpyAsync(&c, tunes_.match.tc, sizeof c, cudaMemcpyDeviceToHost, stream_));
         NSSB_CUDA(cudaStreamSynchronize(stream_));
@@ -241,25 +294,25 @@ void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
 }
 
 // One stage over the planes of a frame (radius 0), one launch per kernel and shape.
-void Engine::run_stage(StageItem* items, int n) {
+void Engine::run_stage(Slot& s, StageItem* items, int n) {
     StagePlane planes[3];
     for (int i = 0; i < n; ++i) {
         const StageItem& it = items[i];
         planes[i] = StagePlane{it.sp, it.src, it.sstride, it.ref, it.rstride, it.dst, it.dstride,
-                               cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], acc_[it.plane], &scratch_[it.plane],
+                               cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], s.acc[it.plane], &s.scratch[it.plane],
                                it.shared_pos, it.shared_count};
     }
-    Clock clock(this);
-    run_stage_planes(planes, n, stream_, tunes_, clock, *tables_);
+    Clock clock(this, &s);
+    run_stage_planes(planes, n, s.stream, tunes_, clock, s.tables);
 }
 
-void Engine::spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory) {
+void Engine::spatial_frame(Slot& s, int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory) {
     const float* src[3]{};
     const float* rp[3]{};
     int64_t ss[3]{}, rs[3]{};
     for (int p = 0; p < cfg_.planes; ++p) {
-        src[p] = device_input(p, clip, first, n, memory, false, &ss[p]);
-        if (cfg_.has_ref) rp[p] = device_input(p, ref, first, n, memory, true, &rs[p]);
+        src[p] = device_input(s, p, clip, first, n, memory, false, &ss[p]);
+        if (cfg_.has_ref) rp[p] = device_input(s, p, ref, first, n, memory, true, &rs[p]);
     }
     StageItem items[3];
     const int np = cfg_.planes;
@@ -270,40 +323,39 @@ void Engine::spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref,
         if (sps[0].sigma == 0.f) {
             const StageParams& s0 = sps[0];
             const int w = cfg_.plane_w[0], h = cfg_.plane_h[0];
-            StageScratch& sc = scratch_[0];
-            timed(kMatch, [&] {
+            StageScratch& sc = s.scratch[0];
+            timed(s, kMatch, [&] {
                 launch_match_spatial(wiener ? items[0].ref : items[0].src, wiener ? items[0].rstride : items[0].sstride,
                                      w, h, s0.block, s0.step, s0.bm_range, s0.group, sc.pos, sc.dist, sc.count,
-                                     stream_);
+                                     s.stream);
             });
         }
         for (int p = 1; p < np; ++p) {
-            items[p].shared_pos = scratch_[0].pos;
-            items[p].shared_count = scratch_[0].count;
+            items[p].shared_pos = s.scratch[0].pos;
+            items[p].shared_count = s.scratch[0].count;
         }
     };
     if (cfg_.two_stage) {
         for (int p = 0; p < np; ++p)
-            items[p] = StageItem{p, &cfg_.basic_stage[p], src[p], ss[p], nullptr, 0, basic_[p].p, basic_[p].pitch};
+            items[p] = StageItem{p, &cfg_.basic_stage[p], src[p], ss[p], nullptr, 0, s.basic[p].p, s.basic[p].pitch};
         chroma_link(cfg_.basic_stage, false);
-        run_stage(items, np);
+        run_stage(s, items, np);
         for (int p = 0; p < np; ++p)
-            items[p] = StageItem{p, &cfg_.final_stage[p], src[p], ss[p], basic_[p].p, basic_[p].pitch, out_[p].p,
-                                 out_[p].pitch};
+            items[p] = StageItem{p, &cfg_.final_stage[p], src[p], ss[p], s.basic[p].p, s.basic[p].pitch, s.out[p].p,
+                                 s.out[p].pitch};
         chroma_link(cfg_.final_stage, true);
-        run_stage(items, np);
+        run_stage(s, items, np);
     } else {
         for (int p = 0; p < np; ++p)
             items[p] = StageItem{p, &cfg_.final_stage[p], src[p], ss[p], cfg_.has_ref ? rp[p] : nullptr, rs[p],
-                                 out_[p].p, out_[p].pitch};
+                                 s.out[p].p, s.out[p].pitch};
         chroma_link(cfg_.final_stage, cfg_.has_ref);
-        run_stage(items, np);
+        run_stage(s, items, np);
     }
 }
 
 void Engine::get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
                        nssb_frame_out* out) {
-    std::lock_guard<std::mutex> lock(mu_);
     NSSB_CUDA(cudaSetDevice(device_));
     if (n < 0 || n >= cfg_.vi.num_frames) throw std::out_of_range("nss_cuda.BM3D: frame number out of range");
     int wf = 0, wl = 0;
@@ -311,20 +363,37 @@ void Engine::get_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int
     if (first > wf || first + count - 1 < wl) throw std::out_of_range("nss_cuda.BM3D: input frames do not cover the window");
     if (cfg_.has_ref && !ref) throw std::invalid_argument("nss_cuda.BM3D: ref frames missing");
     if (cfg_.radius > 0) {
+        std::lock_guard<std::mutex> lock(mu_);
+        Slot* s = lease(true);
+        struct Back {
+            Engine* e;
+            Slot* s;
+            ~Back() { e->give_back(s); }
+        } back{this, s};
         temporal_frame(n, clip, ref, first, count, memory, out);
-        collect_timing();
+        collect_timing(*s);
         return;
     }
-    spatial_frame(n, clip, ref, first, memory);
+    // radius 0: any free slot; frames on different slots overlap
+    Slot* s = lease(false);
+    struct Back {
+        Engine* e;
+        Slot* s;
+        ~Back() {
+            (void)cudaStreamSynchronize(s->stream);  // an error path leaves nothing queued on the slot
+            e->give_back(s);
+        }
+    } back{this, s};
+    spatial_frame(*s, n, clip, ref, first, memory);
     for (int p = 0; p < cfg_.planes; ++p) {
-        const DevPlane& o = out_[p];
+        const DevPlane& o = s->out[p];
         NSSB_CUDA(cudaMemcpy2DAsync(out->planes[p], out->strides[p] * sizeof(float), o.p, o.pitch * sizeof(float),
                                     o.w * sizeof(float), o.h,
                                     memory == NSSB_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                    stream_));
+                                    s->stream));
     }
-    NSSB_CUDA(cudaStreamSynchronize(stream_));
-    collect_timing();
+    NSSB_CUDA(cudaStreamSynchronize(s->stream));
+    collect_timing(*s);
 }
 
 void Engine::plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,

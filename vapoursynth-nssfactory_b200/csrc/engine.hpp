@@ -10,6 +10,7 @@
 #include "params.hpp"
 #include "stage.hpp"
 
+#include <condition_variable>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -78,35 +79,59 @@ public:
     static void plane_stage(const float* src, const float* ref, float* dst, int64_t stride, int w, int h,
                             const StageParams& sp, cudaStream_t stream);
 
+    // Slots the engine renders radius-0 frames on (num_streams).
+    int slots() const { return (int)slots_.size(); }
+
 private:
     struct Plan;
+    // The buffers and stream of one frame in flight -- the reference's slots
+    // (SlotPool, src/cuda/runtime/stream_pool.hpp:62-140; num_streams,
+    // src/cuda/runtime/context.hpp:17-23). A radius-0 frame leases a free
+    // slot for the whole call, so frames requested from several host threads
+    // (VapourSynth's frame threads) overlap: one frame's copies and another's
+    // kernels run on different streams. Temporal frames carry rolling state
+    // from frame to frame and run on slot 0 under the engine lock.
+    struct Slot {
+        cudaStream_t stream = nullptr;
+        DevPlane in[3], refin[3], basic[3], out[3];
+        AccPlane acc[3];
+        StageScratch scratch[3];
+        StageTables tables;
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;  // timing pool
+        std::vector<std::pair<int, size_t>> pending;               // (kind, event pair index)
+        bool busy = false;
+    };
     void alloc();
+    void alloc_slot(Slot& s);
     void release();
-    const float* device_input(int plane, const nssb_frame* frames, int first, int n, int memory, bool is_ref,
-                              int64_t* stride);
-    void spatial_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory);
+    Slot* lease(bool primary);
+    void give_back(Slot* s);
+    const float* device_input(Slot& s, int plane, const nssb_frame* frames, int first, int n, int memory,
+                              bool is_ref, int64_t* stride);
+    void spatial_frame(Slot& s, int n, const nssb_frame* clip, const nssb_frame* ref, int first, int memory);
     // Runs one stage over several planes: one launch per kernel and shape.
-    void run_stage(StageItem* items, int n);
+    void run_stage(Slot& s, StageItem* items, int n);
     void temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref, int first, int count, int memory,
                         nssb_frame_out* out);
 
     using Kind = StageClock::Kind;
     static constexpr Kind kMatch = StageClock::kMatch, kGroup = StageClock::kGroup, kFinish = StageClock::kFinish;
-    void clock_begin(Kind kind);
-    void clock_end(Kind kind);
+    void clock_begin(Slot& s, Kind kind);
+    void clock_end(Slot& s, Kind kind);
     template <class F>
-    void timed(Kind kind, F&& launch) {
-        clock_begin(kind);
+    void timed(Slot& s, Kind kind, F&& launch) {
+        clock_begin(s, kind);
         launch();
-        clock_end(kind);
+        clock_end(s, kind);
     }
-    void collect_timing();
+    void collect_timing(Slot& s);
     void count_match(int w, int h, const StageParams& sp);
     struct Clock : StageClock {
         Engine* e;
-        explicit Clock(Engine* en) : e(en) {}
-        void begin(Kind k) override { e->clock_begin(k); }
-        void end(Kind k) override { e->clock_end(k); }
+        Slot* s;
+        Clock(Engine* en, Slot* sl) : e(en), s(sl) {}
+        void begin(Kind k) override { e->clock_begin(*s, k); }
+        void end(Kind k) override { e->clock_end(*s, k); }
         void count_match(int w, int h, const StageParams& sp) override { e->count_match(w, h, sp); }
     };
 
@@ -114,16 +139,14 @@ private:
     int device_ = 0;
     bool timing_ = false;
     nssb_kernel_stats stats_{};
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool_;
-    std::vector<std::pair<int, size_t>> pending_;  // (kind, event pair index)
-    cudaStream_t stream_ = nullptr;
-    std::mutex mu_;
-    DevPlane in_[3], refin_[3], basic_[3], out_[3];
-    AccPlane acc_[3];
-    StageScratch scratch_[3];
-    std::unique_ptr<StageTables> tables_;
+    std::mutex stats_mu_;                        // stats_, timing_ and the tensor-core counters
+    std::vector<std::unique_ptr<Slot>> slots_;   // slot 0 also serves temporal frames
+    std::mutex slot_mu_;
+    std::condition_variable slot_cv_;
+    cudaStream_t stream_ = nullptr;              // slot 0's stream (the temporal drivers')
+    std::mutex mu_;                              // temporal frames, matcher changes
     LaunchTunes tunes_;
-    Clock clock_{this};
+    std::unique_ptr<Clock> clock_;               // slot 0's accounting (the temporal drivers')
     std::vector<void*> allocations_;
     struct PlanDeleter {
         void operator()(Plan* p) const;

@@ -437,7 +437,7 @@ void Engine::reset_clip(int num_frames) {
 
 size_t Engine::footprint(const Bm3dConfig& cfg, bool host_frames) {
     auto px = [&](int p) { return (size_t)((cfg.plane_w[p] + 31) / 32 * 32) * cfg.plane_h[p]; };
-    size_t total = 0, frame = 0;
+    size_t total = 0, frame = 0, slot = 0;
     const int r = cfg.radius;
     for (int p = 0; p < cfg.planes; ++p) {
         frame += px(p) * 4;
@@ -448,14 +448,16 @@ size_t Engine::footprint(const Bm3dConfig& cfg, bool host_frames) {
             group = std::max(group, (size_t)sp->group);
             cube = std::max(cube, group_filter_scratch_floats(sp->block, sp->group, true));
         }
-        // in, refin, basic, out + num, wsum + pos, slot, dist, count, cube
-        total += px(p) * (4 * 4 + 2 * 8) + jobs * group * 12 + jobs * 4 + cube * 4;
+        // per slot: in, refin, basic, out + num, wsum + pos, slot, dist, count, cube
+        slot += px(p) * (4 * 4 + 2 * 8) + jobs * group * 12 + jobs * 4 + cube * 4;
         if (r > 0) {
             // per temporal stage: 2r+1 target sums + match lists
             const size_t stage = (2 * r + 1) * px(p) * 16 + jobs * group * 12 + jobs * 4 + cube * 4;
             total += stage * (cfg.two_stage ? 2 : 1);
         }
     }
+    // radius 0 renders on num_streams slots, temporal frames on one
+    total += slot * (size_t)(r > 0 ? 1 : std::max(1, cfg.num_streams));
     if (r > 0) {
         size_t frames = cfg.two_stage ? 2 * r + 2 : 0;
         if (host_frames) frames += 8 * r + 2 + (cfg.has_ref ? 4 * r + 2 : 0);
@@ -470,9 +472,9 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
     if (!plan_) {
         plan_.reset(new Plan());
         const bool wiener_final = cfg_.two_stage || cfg_.has_ref;
-        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_, &tunes_.match, &clock_);
+        plan_->final = std::make_unique<TemporalStage>(cfg_, cfg_.final_stage, wiener_final, stream_, &tunes_.match, clock_.get());
         if (cfg_.two_stage) {
-            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_, &tunes_.match, &clock_);
+            plan_->basic = std::make_unique<TemporalStage>(cfg_, cfg_.basic_stage, false, stream_, &tunes_.match, clock_.get());
             plan_->basic_cache = std::make_unique<FrameCache>(cfg_, 2 * r + 2, stream_);
         }
     }
@@ -525,8 +527,8 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
     int64_t dstride[3]{};
     if (cfg_.rolling) {
         for (int p = 0; p < cfg_.planes; ++p) {
-            dst[p] = host_out ? out_[p].p : out->planes[p];
-            dstride[p] = host_out ? out_[p].pitch : out->strides[p];
+            dst[p] = host_out ? slots_[0]->out[p].p : out->planes[p];
+            dstride[p] = host_out ? slots_[0]->out[p].pitch : out->strides[p];
         }
         plan_->final->render(n, src, final_ref, dst, dstride);
         if (host_out) {
@@ -541,7 +543,7 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
     std::vector<void*> tmp;
     for (int p = 0; p < cfg_.planes; ++p) {
         if (host_out) {
-            dstride[p] = out_[p].pitch;
+            dstride[p] = slots_[0]->out[p].pitch;
             dst[p] = static_cast<float*>(dev_alloc((size_t)dstride[p] * cfg_.plane_h[p] * (2 * r + 1) * 2 * 4));
             tmp.push_back(dst[p]);
         } else {
@@ -567,7 +569,8 @@ void Engine::temporal_frame(int n, const nssb_frame* clip, const nssb_frame* ref
 }
 
 Engine::~Engine() {
-    if (stream_) (void)cudaStreamSynchronize(stream_);
+    for (auto& s : slots_)
+        if (s->stream) (void)cudaStreamSynchronize(s->stream);
     plan_.reset();
     release();
 }
