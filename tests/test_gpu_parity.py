@@ -60,7 +60,10 @@ SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 
           # large windows (bm_range 16 and up: the window spans most of the test image);
           # the 8x8 fast path covers up to 31
           (8, 8, 8, 25), (8, 4, 4, 25), (8, 8, 16, 16), (8, 6, 2, 16), (8, 4, 16, 32), (4, 3, 8, 40),
-          (16, 8, 8, 64)]
+          (16, 8, 8, 64),
+          # groups of 32 on the 8x8 matcher (the list split over a reference's two lanes),
+          # the "heavy" preset's range 19 (its own kernel) among them
+          (8, 3, 32, 19), (8, 4, 32, 9), (8, 8, 32, 25), (8, 2, 32, 12), (8, 5, 16, 19), (8, 1, 32, 6)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", SHAPES)
@@ -79,7 +82,8 @@ def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_)
         assert [m[3] for m in om] == [float(v) for v in dist[j, :len(om)]]
 
 
-@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16), (20, 8), (30, 4), (11, 8)])
+@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16), (20, 8), (30, 4), (11, 8), (19, 32), (19, 16),
+                                        (31, 32)])
 def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group):
     # windows well inside a larger plane (most references see the whole window)
     noisy, _ = synth.gray_frame(17, 256, 160, sigma=10)
@@ -126,7 +130,7 @@ def gpu_stage(nssb, src, ref, st, dev):
 
 STAGES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (16, 8, 16, 7), (12, 6, 8, 5), (2, 2, 4, 4), (1, 1, 2, 3),
           (32, 16, 8, 3), (8, 3, 32, 7), (16, 8, 64, 5), (32, 16, 32, 4), (8, 8, 16, 25), (8, 4, 8, 32),
-          (8, 8, 8, 16)]
+          (8, 8, 8, 16), (8, 3, 32, 19), (8, 8, 32, 9), (8, 3, 16, 19)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", STAGES)

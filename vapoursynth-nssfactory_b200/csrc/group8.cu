@@ -1,9 +1,10 @@
-// Collaborative filtering for 8x8 blocks and groups of 4, 8 or 16 (sm_100a):
+// Collaborative filtering for 8x8 blocks and groups of 4, 8, 16 or 32 (sm_100a):
 // the default BM3D shapes. Same semantics as group.cu (the reference's
 // Bm3dFilterGroup, src/cpu/bm/dct8.cpp:926-1133); the schedule is one warp
 // per group, the cube in registers and a padded per-warp shared buffer:
 //   - 32/G lanes per patch, each holding 8G/32 rows, then as many columns,
 //     then two Haar tubes (coefficient positions l and l+32 across the group);
+//     with 32 patches (the "heavy" final stage) a lane holds a whole patch;
 //   - the per-patch stride is 64 + 32/G floats and a coefficient's column is
 //     XORed with its row's owner lane, so the row, column and tube phases of
 //     the 32 lanes each touch 32 different banks;
@@ -106,6 +107,17 @@ __device__ __forceinline__ void haar_inv(float* t) {
 }
 
 constexpr int kWarps = 4;
+
+// Warps per CTA: the requested count, or fewer where the per-warp cubes (the
+// reference cube too for Wiener) would exceed 48 KB of static shared memory
+// (groups of 32: 8.3 KB per cube).
+template <int G, bool WIENER>
+__host__ __device__ constexpr int warps_fit(int want) {
+    const int bytes = G * (64 + 32 / G) * 4 * (WIENER ? 2 : 1);
+    int w = want;
+    while (w > 1 && w * bytes > 48 * 1024) w /= 2;
+    return w;
+}
 
 template <int G>
 struct Shape {
@@ -313,20 +325,20 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 }
 
 // Temporal / single-plane form: slots of GroupIO.
-template <int G, bool WIENER>
-__global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const int32_t* __restrict__ pos,
-                                                             const int32_t* __restrict__ slot,
-                                                             const int32_t* __restrict__ count, int njobs,
-                                                             float sigma) {
+template <int G, bool WIENER, int NW = warps_fit<G, WIENER>(kWarps)>
+__global__ void __launch_bounds__(32 * NW) group8_kernel(GroupIO io, const int32_t* __restrict__ pos,
+                                                         const int32_t* __restrict__ slot,
+                                                         const int32_t* __restrict__ count, int njobs,
+                                                         float sigma) {
     using Sh = Shape<G>;
     constexpr int CUBE = G * Sh::S;
-    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    __shared__ float smem[NW][WIENER ? 2 * CUBE : CUBE];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / Sh::LP;
-    const int stride_w = gridDim.x * kWarps;
+    const int stride_w = gridDim.x * NW;
     bool vec = io.stride % 4 == 0 && io.ref_stride % 4 == 0;
     for (int q = 0; q < kMaxSlots; ++q) vec = vec && aligned16(io.src[q]) && aligned16(io.ref[q]);
-    for (int job = blockIdx.x * kWarps + warp; job < njobs; job += stride_w) {
+    for (int job = blockIdx.x * NW + warp; job < njobs; job += stride_w) {
         const int k = count[job];
         if (k <= 0) continue;
         const int32_t p = g < k ? pos[(size_t)job * G + g] : 0;
@@ -349,14 +361,14 @@ __global__ void __launch_bounds__(32 * kWarps) group8_kernel(GroupIO io, const i
 // Temporal centre, batched over its planes: each plane with its own slots;
 // the next job's count, positions and slots are read ahead as in the
 // batched form below.
-template <int G, bool WIENER>
-__global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const __grid_constant__ GroupSlotBatch gb) {
+template <int G, bool WIENER, int NW = warps_fit<G, WIENER>(kWarps)>
+__global__ void __launch_bounds__(32 * NW) group8_slots_batch_kernel(const __grid_constant__ GroupSlotBatch gb) {
     using Sh = Shape<G>;
     constexpr int CUBE = G * Sh::S;
-    __shared__ float smem[kWarps][WIENER ? 2 * CUBE : CUBE];
+    __shared__ float smem[NW][WIENER ? 2 * CUBE : CUBE];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / Sh::LP;
-    const int stride_w = gridDim.x * kWarps;
+    const int stride_w = gridDim.x * NW;
     // planes whose every slot row is 16-byte aligned
     int vec_mask = 0;
     for (int q = 0; q < gb.n; ++q) {
@@ -375,7 +387,7 @@ __global__ void __launch_bounds__(32 * kWarps) group8_slots_batch_kernel(const _
         s = (P_.slot && g < k) ? P_.slot[(size_t)lj * G + g] : 0;
         plane = pl;
     };
-    int job = blockIdx.x * kWarps + warp;
+    int job = blockIdx.x * NW + warp;
     int k = 0, s = 0, plane = 0;
     int32_t p = 0;
     if (job < gb.total_jobs) fetch(job, k, p, s, plane);
@@ -459,8 +471,9 @@ __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_cons
 template <int G, bool W>
 void launch_gw(const GroupIO& io, const int32_t* pos, const int32_t* slot, const int32_t* count, int njobs,
                float sigma, cudaStream_t stream) {
-    const int blocks = std::min(ceil_div(njobs, kWarps), 148 * 16);
-    group8_kernel<G, W><<<blocks, 32 * kWarps, 0, stream>>>(io, pos, slot, count, njobs, sigma);
+    constexpr int NW = warps_fit<G, W>(kWarps);
+    const int blocks = std::min(ceil_div(njobs, NW), 148 * 16);
+    group8_kernel<G, W><<<blocks, 32 * NW, 0, stream>>>(io, pos, slot, count, njobs, sigma);
     NSSB_CUDA(cudaGetLastError());
 }
 
@@ -479,14 +492,11 @@ void launch_batch_gwn(const GroupBatch& gb, int ctas_per_sm, cudaStream_t stream
 
 template <int G, bool W>
 void launch_batch_gw(const GroupBatch& gb, const GroupTune& t, cudaStream_t stream) {
+    // the requested warps per CTA, fewer where the cubes would not fit
     switch (t.warps) {
-        case 2: launch_batch_gwn<G, W, 2>(gb, t.ctas_per_sm, stream); break;
-        case 8:
-            // 8 Wiener cubes of 16 patches exceed the 48 KB of static shared memory
-            if constexpr (G == 16 && W) launch_batch_gwn<G, W, 4>(gb, t.ctas_per_sm, stream);
-            else launch_batch_gwn<G, W, 8>(gb, t.ctas_per_sm, stream);
-            break;
-        default: launch_batch_gwn<G, W, 4>(gb, t.ctas_per_sm, stream); break;
+        case 2: launch_batch_gwn<G, W, warps_fit<G, W>(2)>(gb, t.ctas_per_sm, stream); break;
+        case 8: launch_batch_gwn<G, W, warps_fit<G, W>(8)>(gb, t.ctas_per_sm, stream); break;
+        default: launch_batch_gwn<G, W, warps_fit<G, W>(4)>(gb, t.ctas_per_sm, stream); break;
     }
 }
 
@@ -508,6 +518,10 @@ bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, c
             wiener ? launch_gw<16, true>(io, pos, slot, count, njobs, sigma, stream)
                    : launch_gw<16, false>(io, pos, slot, count, njobs, sigma, stream);
             return true;
+        case 32:
+            wiener ? launch_gw<32, true>(io, pos, slot, count, njobs, sigma, stream)
+                   : launch_gw<32, false>(io, pos, slot, count, njobs, sigma, stream);
+            return true;
         default:
             return false;
     }
@@ -515,9 +529,12 @@ bool launch_group8(const GroupIO& io, const int32_t* pos, const int32_t* slot, c
 
 bool launch_group8_slots_batch(const GroupSlotBatch& gb, int group, bool wiener, cudaStream_t stream) {
     if (gb.total_jobs <= 0) return true;
-    const int blocks = std::min(ceil_div(gb.total_jobs, kWarps), 148 * 16);
     auto go = [&](auto kern) {
-        kern<<<blocks, 32 * kWarps, 0, stream>>>(gb);
+        cudaFuncAttributes fa{};
+        NSSB_CUDA(cudaFuncGetAttributes(&fa, kern));
+        const int nw = fa.maxThreadsPerBlock >= 32 * kWarps ? kWarps : fa.maxThreadsPerBlock / 32;
+        const int blocks = std::min(ceil_div(gb.total_jobs, nw), 148 * 16);
+        kern<<<blocks, 32 * nw, 0, stream>>>(gb);
         NSSB_CUDA(cudaGetLastError());
     };
     switch (group) {
@@ -525,6 +542,9 @@ bool launch_group8_slots_batch(const GroupSlotBatch& gb, int group, bool wiener,
         case 8: wiener ? go(group8_slots_batch_kernel<8, true>) : go(group8_slots_batch_kernel<8, false>); return true;
         case 16:
             wiener ? go(group8_slots_batch_kernel<16, true>) : go(group8_slots_batch_kernel<16, false>);
+            return true;
+        case 32:
+            wiener ? go(group8_slots_batch_kernel<32, true>) : go(group8_slots_batch_kernel<32, false>);
             return true;
         default: return false;
     }
@@ -538,6 +558,9 @@ bool launch_group8_batch(const GroupBatch& gb, int group, bool wiener, cudaStrea
         case 8: wiener ? launch_batch_gw<8, true>(gb, t, stream) : launch_batch_gw<8, false>(gb, t, stream); return true;
         case 16:
             wiener ? launch_batch_gw<16, true>(gb, t, stream) : launch_batch_gw<16, false>(gb, t, stream);
+            return true;
+        case 32:
+            wiener ? launch_batch_gw<32, true>(gb, t, stream) : launch_batch_gw<32, false>(gb, t, stream);
             return true;
         default: return false;
     }

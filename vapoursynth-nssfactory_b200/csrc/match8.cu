@@ -1,6 +1,7 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape
 // (bm_range 9), and every range from 4 to 31 (kernels built for 4-9, 12,
-// 15, 16, 25 and 31; a range between two runs on the larger one).
+// 15, 16, 19, 25 and 31; a range between two runs on the larger one), groups
+// of 2, 4, 8, 16 and 32.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
 // keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
@@ -21,8 +22,8 @@
 //     (__ffma2_rn) carries two block columns per instruction, so a row costs 4
 //     shared loads and 32 packed operations per lane. A finished candidate's
 //     two half sums meet through one shuffle; the sum enters the reference's
-//     register top-k, kept identically by both lanes; the P partial lists
-//     merge in shared memory.
+//     register top-k, kept identically by both lanes (split over the two
+//     lanes for groups of 32); the P partial lists merge in shared memory.
 #include "kernels.cuh"
 
 #include <algorithm>
@@ -39,24 +40,73 @@ __device__ __forceinline__ uint64_t key_of(float d, int x, int y) {
     return (uint64_t(b) << 32) | (uint64_t(uint32_t(y)) << 16) | uint64_t(uint32_t(x));
 }
 
+// Inserts v into the sorted list k[0..S) if it beats the last entry; returns
+// what leaves the list (the old last entry, or v itself). All S comparisons
+// first (independent), then every slot takes its own entry, the one before
+// it, or v: no chain through the list.
+template <int S>
+__device__ __forceinline__ uint64_t sorted_insert(uint64_t* k, uint64_t v) {
+    const uint64_t last = k[S - 1];
+    if (!(v < last)) return v;
+    bool c[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) c[q] = v < k[q];
+#pragma unroll
+    for (int q = S - 1; q > 0; --q) k[q] = c[q] ? (c[q - 1] ? k[q - 1] : v) : k[q];
+    k[0] = c[0] ? v : k[0];
+    return last;
+}
+
+// The K best keys of a reference, kept identically by both lanes of it.
 template <int K>
 struct TopK {
+    static constexpr int kHeld = K;  // list entries in each lane
     uint64_t k[K];
-    __device__ __forceinline__ void init() {
+    __device__ __forceinline__ void init(int) {
 #pragma unroll
         for (int q = 0; q < K; ++q) k[q] = ~0ull;
     }
-    // all K comparisons first (independent), then every slot takes its own
-    // entry, the one before it, or v: no chain through the list
-    __device__ __forceinline__ void add(uint64_t v) {
-        if (!(v < k[K - 1])) return;
-        bool c[K];
+    __device__ __forceinline__ void add(uint64_t v) { (void)sorted_insert<K>(k, v); }
+    __device__ __forceinline__ uint64_t worst() const { return k[K - 1]; }
+    // entry q of the list, and whether this lane holds it
+    __device__ __forceinline__ bool holds(int q, int half) const { return half == 0; }
+    __device__ __forceinline__ uint64_t at(int q) const { return k[q]; }
+};
+
+// Groups of 32: the 31-entry list split over the two lanes of a reference
+// (half 0 the 16 smallest keys, half 1 the next 15), so a lane holds no more
+// registers than the 15-entry list. Both lanes offer every key: half 0 puts
+// it into its list when it beats that list's last entry, and what leaves
+// half 0's list (or the key) goes on to half 1's; both lanes then take the
+// overall worst from half 1, so they agree on every pass mask and run the
+// same insertions (the pair's shuffles use the pair's own lane mask).
+template <int K>
+struct SplitTopK {
+    static constexpr int LO = (K + 1) / 2, HI = K - LO, kHeld = LO;
+    uint64_t k[LO];
+    uint64_t worst_;
+    int half, lo_lane, hi_lane;
+    unsigned pair;
+    __device__ __forceinline__ void init(int lane) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) c[q] = v < k[q];
-#pragma unroll
-        for (int q = K - 1; q > 0; --q) k[q] = c[q] ? (c[q - 1] ? k[q - 1] : v) : k[q];
-        k[0] = c[0] ? v : k[0];
+        for (int q = 0; q < LO; ++q) k[q] = ~0ull;
+        worst_ = ~0ull;
+        half = lane >> 4;
+        lo_lane = lane & 15;
+        hi_lane = lo_lane | 16;
+        pair = (1u << lo_lane) | (1u << hi_lane);
     }
+    __device__ __forceinline__ void add(uint64_t v) {
+        if (!(v < worst_)) return;  // the same decision in both lanes
+        uint64_t up = v;
+        if (half == 0) up = sorted_insert<LO>(k, v);
+        up = __shfl_sync(pair, up, lo_lane);  // what half 0 let go, in both lanes
+        if (half == 1) (void)sorted_insert<HI>(k, up);
+        worst_ = __shfl_sync(pair, k[HI - 1], hi_lane);
+    }
+    __device__ __forceinline__ uint64_t worst() const { return worst_; }
+    __device__ __forceinline__ bool holds(int q, int h) const { return h == (q < LO ? 0 : 1); }
+    __device__ __forceinline__ uint64_t at(int q) const { return k[q < LO ? q : q - LO]; }
 };
 
 constexpr int kLanes = 32;   // references per CTA
@@ -151,8 +201,9 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
             ref[i][h] = make_float2(tile[(R + i) * kPitch + swz(tc0 + R + 2 * h)],
                                     tile[(R + i) * kPitch + swz(tc0 + R + 2 * h + 1)]);
 
-    TopK<K> topk;
-    topk.init();
+    using List = typename std::conditional<(K > 15), SplitTopK<K>, TopK<K>>::type;
+    List topk;
+    topk.init(lane);
     // finished distances of the current column, one slot per candidate row:
     // an emit stores its sum and marks a bit when it may enter the list; the
     // insertions run after the column, once per marked candidate
@@ -171,7 +222,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
         Mask pass = 0;
         // a candidate may enter unless it is farther than the current worst
         // (NaN never compares greater: non-finite sums always take the exact path)
-        const float worst = __uint_as_float(uint32_t(topk.k[K - 1] >> 32));
+        const float worst = __uint_as_float(uint32_t(topk.worst() >> 32));
         int col[HB];
 #pragma unroll
         for (int j = 0; j < HB; ++j) col[j] = swz(tc0 + dxi + j);
@@ -217,9 +268,10 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     if constexpr (P > 1) {
         __syncthreads();
         uint64_t* keys = reinterpret_cast<uint64_t*>(tile);  // [P][K][32 references]
-        if (part > 0 && half == 0) {
+        if (part > 0) {
 #pragma unroll
-            for (int q = 0; q < K; ++q) keys[(part * K + q) * kLanes + l] = topk.k[q];
+            for (int q = 0; q < K; ++q)
+                if (topk.holds(q, half)) keys[(part * K + q) * kLanes + l] = topk.at(q);
         }
         __syncthreads();
         if (part > 0) return;
@@ -227,26 +279,29 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
 #pragma unroll
             for (int q = 0; q < K; ++q) topk.add(keys[(w * K + q) * kLanes + l]);
     }
-    if (!active || half != 0) return;
+    // each lane writes the entries it holds; the pair adds up the count
+    int n = 0;
+#pragma unroll
+    for (int q = 0; q < K; ++q) n += (topk.holds(q, half) && topk.at(q) != ~0ull) ? 1 : 0;
+    n += __shfl_xor_sync(0xffffffffu, n, 16);
+    if (!active) return;
     const int64_t job = (int64_t)ry * nx + rx;
     constexpr int G = K + 1;
     int32_t* op = P_.pos + job * G;
-    op[0] = pack_pos(cx, cy);
-    int n = 0;
+    float* od = P_.dist ? P_.dist + job * G : nullptr;
+    if (half == 0) {
+        op[0] = pack_pos(cx, cy);
+        if (od) od[0] = 0.f;
+        P_.count[job] = 1 + n;
+    }
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        const bool valid = topk.k[q] != ~0ull;
-        n += valid;
-        op[1 + q] = valid ? int32_t(uint32_t(topk.k[q])) : -1;
+        if (!topk.holds(q, half)) continue;
+        const uint64_t e = topk.at(q);
+        const bool valid = e != ~0ull;
+        op[1 + q] = valid ? int32_t(uint32_t(e)) : -1;
+        if (od) od[1 + q] = valid ? __uint_as_float(uint32_t(e >> 32)) : 0.f;
     }
-    if (P_.dist) {
-        float* od = P_.dist + job * G;
-        od[0] = 0.f;
-#pragma unroll
-        for (int q = 0; q < K; ++q)
-            od[1 + q] = topk.k[q] != ~0ull ? __uint_as_float(uint32_t(topk.k[q] >> 32)) : 0.f;
-    }
-    P_.count[job] = 1 + n;
 }
 
 // Grid form: CTA b takes tile b. Persistent form (mb.queue set): a CTA takes
@@ -323,6 +378,7 @@ bool launch_r(MatchBatch& mb, int group, const MatchTune& tune, cudaStream_t str
         case 4: launch_rk<R, 3>(mb, tune, stream); return true;
         case 8: launch_rk<R, 7>(mb, tune, stream); return true;
         case 16: launch_rk<R, 15>(mb, tune, stream); return true;
+        case 32: launch_rk<R, 31>(mb, tune, stream); return true;
         default: return false;
     }
 }
@@ -352,6 +408,7 @@ bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t s
     if (bm_range <= 12) return launch_r<12>(mb, group, t, stream);
     if (bm_range <= 15) return launch_r<15>(mb, group, t, stream);
     if (bm_range <= 16) return launch_r<16>(mb, group, t, stream);
+    if (bm_range <= 19) return launch_r<19>(mb, group, t, stream);
     if (bm_range <= 25) return launch_r<25>(mb, group, t, stream);
     if (bm_range <= 31) return launch_r<31>(mb, group, t, stream);
     return false;

@@ -310,7 +310,7 @@ private:
             io.ref_stride = rstride;
             io.acc_stride = pitch_[p];
             const int jobs = grid_count(w, st.block, st.step) * grid_count(h, st.block, st.step);
-            const bool fits = st.block == 8 && (st.group == 4 || st.group == 8 || st.group == 16) &&
+            const bool fits = st.block == 8 && (st.group == 4 || st.group == 8 || st.group == 16 || st.group == 32) &&
                               (gshape < 0 || gshape == st.group);
             if (batchable && fits) {
                 gshape = st.group;
