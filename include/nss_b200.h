@@ -150,6 +150,18 @@ int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stat
 #define NSSB_MATCHER_TENSOR 1
 int nssb_bm3d_set_matcher(nssb_bm3d* h, int form);
 
+/* Opt-in Kaiser aggregation window. No counterpart in the reference's BM3D,
+ * whose aggregation weights every pixel of a group's patches by one flat
+ * per-group weight (src/cpu/bm/dct8.cpp:1126-1131,
+ * src/cuda/bm3d/kernels.cu:292-301); the reference windows only its BM4D
+ * (src/cuda/bm4d/kernels.cu:734). With beta > 0 each patch pixel (i, j) is
+ * weighted by w * K(i) K(j), K(n) = I0(beta sqrt(1 - (2n/(B-1) - 1)^2)) / I0(beta),
+ * in num and den alike; beta = 0 (the default) is the reference's aggregation
+ * bit for bit. Radius-0 filters rendered by nssb_bm3d_get_frame only
+ * (NSSB_ERR_STATE otherwise; the batched form rejects such nodes). Not
+ * parity-checked against the reference, which has no such mode. */
+int nssb_bm3d_set_window(nssb_bm3d* h, float beta);
+
 /* ---- stage primitives on device memory (the kernels the filter runs) ----
  * Strides are in elements. stream is a cudaStream_t (NULL = default). */
 

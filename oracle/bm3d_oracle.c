@@ -648,14 +648,18 @@ static void pack_patch(float* col, const float* src, ptrdiff_t stride, int x, in
 }
 
 /* UnpackPatch (pack.cpp:42-87) for an in-bounds patch: num = w*v + num (one
- * rounding), den += w. */
-static void unpack_patch(float* num, float* den, int width, int x, int y, const float* col, int block, float w) {
+ * rounding), den += w. With a window (block x block weights, not part of the
+ * reference's BM3D: the opt-in Kaiser mode of this build) every pixel takes
+ * ww = w * win instead of w. */
+static void unpack_patch(float* num, float* den, int width, int x, int y, const float* col, int block, float w,
+                         const float* win) {
     for (int py = 0; py < block; ++py) {
         float* n = num + (ptrdiff_t)(y + py) * width + x;
         float* d = den + (ptrdiff_t)(y + py) * width + x;
         for (int px = 0; px < block; ++px) {
-            n[px] = fmaf(w, col[py * block + px], n[px]);
-            d[px] = d[px] + w;
+            const float ww = win ? w * win[py * block + px] : w;
+            n[px] = fmaf(ww, col[py * block + px], n[px]);
+            d[px] = d[px] + ww;
         }
     }
 }
@@ -674,6 +678,7 @@ typedef struct pass_ctx {
     float* den;
     int slices;
     int radius, t0;
+    const float* win; /* opt-in aggregation window (block x block), or NULL */
 } pass_ctx;
 
 static void filter_commit(pass_ctx* c, const om_match* m, int k, float* cube, float* refcube) {
@@ -690,7 +695,7 @@ static void filter_commit(pass_ctx* c, const om_match* m, int k, float* cube, fl
     for (int j = 0; j < k; ++j) {
         const int sl = c->radius > 0 ? iclamp(m[j].t - c->t0 + c->radius, 0, c->slices - 1) : 0;
         unpack_patch(c->num + sl * plane, c->den + sl * plane, c->width, m[j].x, m[j].y,
-                     cube + (ptrdiff_t)j * area, block, w);
+                     cube + (ptrdiff_t)j * area, block, w, c->win);
     }
 }
 
@@ -709,9 +714,25 @@ int om_bm3d_plane(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff
                                  counts);
 }
 
+static int plane_pass(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride,
+                      const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st, int wiener,
+                      const float* win, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts);
+
 int om_bm3d_plane_matched(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride,
                           const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st,
                           int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts) {
+    return plane_pass(src, sstride, ref, rstride, match, mstride, width, height, st, wiener, NULL, dst, dstride,
+                      matches, counts);
+}
+
+int om_bm3d_plane_window(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width,
+                         int height, const om_stage* st, int wiener, const float* win, float* dst, ptrdiff_t dstride) {
+    return plane_pass(src, sstride, ref, rstride, NULL, 0, width, height, st, wiener, win, dst, dstride, NULL, NULL);
+}
+
+static int plane_pass(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride,
+                      const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st, int wiener,
+                      const float* win, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts) {
     if (st->sigma == 0.f) {
         for (int y = 0; y < height; ++y) memcpy(dst + y * dstride, src + y * sstride, (size_t)width * sizeof(float));
         return 0;
@@ -729,7 +750,7 @@ int om_bm3d_plane_matched(const float* src, ptrdiff_t sstride, const float* ref,
     const float* match_src = match ? match : (wiener ? ref : src);
     const ptrdiff_t match_stride = match ? mstride : (wiener ? rstride : sstride);
     pass_ctx c = {&src, &sstride, wiener ? &ref : NULL, &rstride, width, height, st, wiener,
-                  num, num + plane, 1, 0, 0};
+                  num, num + plane, 1, 0, 0, win};
     const int nx = om_grid_count(width, block, st->step), ny = om_grid_count(height, block, st->step);
     om_match m[OM_MAX_GROUP];
     for (int j = 0; j < ny; ++j) {
@@ -792,7 +813,7 @@ int om_bm3d_plane_fat(const float* const* src, const float* const* ref, int nfra
         return -1;
     }
     pass_ctx c = {srcs, strides, wiener ? refs : NULL, strides, width, height, st, wiener,
-                  num, num + plane * ntemp, ntemp, radius, radius};
+                  num, num + plane * ntemp, ntemp, radius, radius, NULL};
     om_search cfg = {block, st->step, group, st->bm_range, radius, st->ps_num, st->ps_range,
                      imax(0, radius - n), radius + imin(radius + 1, nframes - n)};
     const int nx = om_grid_count(width, block, st->step), ny = om_grid_count(height, block, st->step);

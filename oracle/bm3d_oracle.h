@@ -109,6 +109,13 @@ int om_bm3d_plane_matched(const float* src, ptrdiff_t sstride, const float* ref,
                           const float* match, ptrdiff_t mstride, int width, int height, const om_stage* st,
                           int wiener, float* dst, ptrdiff_t dstride, int32_t* matches, int32_t* counts);
 
+/* om_bm3d_plane with an aggregation window: each patch pixel adds w * win
+ * (block x block weights, row-major) to num (times the value) and den. This
+ * is this build's opt-in Kaiser mode, not the reference's BM3D (whose weights
+ * are flat per group): it checks the device's windowed mode, nothing else. */
+int om_bm3d_plane_window(const float* src, ptrdiff_t sstride, const float* ref, ptrdiff_t rstride, int width,
+                         int height, const om_stage* st, int wiener, const float* win, float* dst, ptrdiff_t dstride);
+
 /* Radius > 0, one plane of a whole clip: each centre c matches predictively
  * over its 2r+1 slots (temporal.hpp:19-21), filters and adds to num/den
  * slices of its target frames; each frame is then reduced over its centres

@@ -68,6 +68,9 @@ def lib():
         L.om_bm3d_plane.restype = C.c_int
         L.om_bm3d_plane.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int, C.POINTER(Stage), C.c_int,
                                     fp, C.c_ssize_t, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.om_bm3d_plane_window.restype = C.c_int
+        L.om_bm3d_plane_window.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int, C.POINTER(Stage),
+                                           C.c_int, fp, fp, C.c_ssize_t]
         L.om_bm3d_plane_matched.restype = C.c_int
         L.om_bm3d_plane_matched.argtypes = [fp, C.c_ssize_t, fp, C.c_ssize_t, fp, C.c_ssize_t, C.c_int, C.c_int,
                                             C.POINTER(Stage), C.c_int, fp, C.c_ssize_t, C.POINTER(C.c_int32),
@@ -182,6 +185,39 @@ def bm3d_plane(src, st: Stage, ref=None, want_matches=False):
         raise RuntimeError("oracle plane pass failed")
     if want_matches:
         return dst, matches, counts
+    return dst
+
+
+def kaiser_window(block: int, beta: float) -> np.ndarray:
+    """block x block Kaiser window (outer product of the 1-D window
+    I0(beta sqrt(1 - (2n/(N-1) - 1)^2)) / I0(beta)), float32; ones at beta 0."""
+    def i0(x):
+        term, s, k = 1.0, 1.0, 1
+        while term > 1e-17 * s:
+            term *= (x / (2.0 * k)) ** 2
+            s += term
+            k += 1
+        return s
+    if block == 1 or beta == 0.0:
+        w1 = np.ones(block)
+    else:
+        n = np.arange(block)
+        r = 2.0 * n / (block - 1) - 1.0
+        w1 = np.array([i0(beta * np.sqrt(max(0.0, 1.0 - v * v))) / i0(beta) for v in r])
+    return np.outer(w1, w1).astype(np.float32)
+
+
+def bm3d_plane_window(src, st: Stage, win: np.ndarray, ref=None) -> np.ndarray:
+    """One radius-0 stage with the opt-in aggregation window (see the C header)."""
+    s = _f32(src)
+    h, w = s.shape
+    r = _f32(ref) if ref is not None else None
+    wn = _f32(win)
+    dst = np.empty_like(s)
+    rc = lib().om_bm3d_plane_window(_fp(s), w, _fp(r) if r is not None else None, w, w, h, C.byref(st),
+                                    int(r is not None), _fp(wn), _fp(dst), w)
+    if rc != 0:
+        raise RuntimeError("oracle windowed pass failed")
     return dst
 
 

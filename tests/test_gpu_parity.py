@@ -63,7 +63,11 @@ SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 
           (16, 8, 8, 64),
           # groups of 32 on the 8x8 matcher (the list split over a reference's two lanes),
           # the "heavy" preset's range 19 (its own kernel) among them
-          (8, 3, 32, 19), (8, 4, 32, 9), (8, 8, 32, 25), (8, 2, 32, 12), (8, 5, 16, 19), (8, 1, 32, 6)]
+          (8, 3, 32, 19), (8, 4, 32, 9), (8, 8, 32, 25), (8, 2, 32, 12), (8, 5, 16, 19), (8, 1, 32, 6),
+          # steps 1-4 on the column-reuse matcher (the last grid column clamped at W = 61
+          # for steps 2-4 goes to the direct one)
+          (8, 1, 8, 9), (8, 2, 16, 16), (8, 3, 8, 25), (8, 4, 8, 31), (8, 3, 4, 12), (8, 1, 16, 19),
+          (8, 2, 4, 10), (8, 4, 32, 19)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", SHAPES)
@@ -82,13 +86,14 @@ def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_)
         assert [m[3] for m in om] == [float(v) for v in dist[j, :len(om)]]
 
 
-@pytest.mark.parametrize("rng_,group", [(16, 8), (25, 16), (20, 8), (30, 4), (11, 8), (19, 32), (19, 16),
-                                        (31, 32)])
-def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group):
+@pytest.mark.parametrize("rng_,group,step", [(16, 8, 8), (25, 16, 8), (20, 8, 8), (30, 4, 8), (11, 8, 8), (19, 32, 8),
+                                             (19, 16, 8), (31, 32, 8), (19, 16, 3), (19, 32, 3), (9, 8, 4),
+                                             (12, 16, 2)])
+def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group, step):
     # windows well inside a larger plane (most references see the whole window)
     noisy, _ = synth.gray_frame(17, 256, 160, sigma=10)
-    pos, dist, cnt = gpu_match(nssb, noisy, block=8, step=8, rng_=rng_, group=group, dev=dev)
-    st = oracle.stage(oracle.effective_sigma(10.0), block=8, group=group, step=8, bm_range=rng_)
+    pos, dist, cnt = gpu_match(nssb, noisy, block=8, step=step, rng_=rng_, group=group, dev=dev)
+    st = oracle.stage(oracle.effective_sigma(10.0), block=8, group=group, step=step, bm_range=rng_)
     _, want, wcnt = oracle.bm3d_plane(noisy, st, want_matches=True)
     assert np.array_equal(cnt, wcnt)
     assert np.array_equal(pos, want)

@@ -172,6 +172,7 @@ def lib():
         L.nssb_bm3d_plane_stage_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                                     C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.nssb_bm3d_set_matcher.argtypes = [C.c_void_p, C.c_int]
+        L.nssb_bm3d_set_window.argtypes = [C.c_void_p, C.c_float]
         L.nssb_bm3d_frame_props.argtypes = [C.c_void_p, C.c_int, C.POINTER(Prop), C.c_int, C.POINTER(C.c_int)]
         L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
@@ -325,6 +326,10 @@ class Node:
     def set_matcher(self, form: int) -> None:
         """0: FP32 matcher (default); 1: tensor-core precision form (identical lists)."""
         check(lib().nssb_bm3d_set_matcher(self.handle, int(form)))
+
+    def set_window(self, beta: float) -> None:
+        """Opt-in Kaiser aggregation window (beta > 0); 0 restores the reference's flat weights."""
+        check(lib().nssb_bm3d_set_window(self.handle, float(beta)))
 
     def frame_window(self, n: int):
         a, b = C.c_int(), C.c_int()

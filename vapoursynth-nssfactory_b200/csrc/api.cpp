@@ -206,6 +206,13 @@ int nssb_bm3d_frame_props(const nssb_bm3d* h, int n, nssb_prop* out, int cap, in
     });
 }
 
+int nssb_bm3d_set_window(nssb_bm3d* h, float beta) {
+    return guarded([&] {
+        if (!h) throw std::invalid_argument("nssb_bm3d_set_window: invalid handle");
+        h->engine->set_window(beta);
+    });
+}
+
 int nssb_bm3d_set_matcher(nssb_bm3d* h, int form) {
     return guarded([&] {
         if (!h) throw std::invalid_argument("nssb_bm3d_set_matcher: invalid handle");

@@ -439,6 +439,8 @@ void BatchEngine::run(const BatchItem* items, int n) {
         const BatchItem& it = items[i];
         if (!it.cfg || !it.clip || !it.out) throw std::invalid_argument("nssb_batch_run: item without node, clip or out");
         if (it.cfg->radius != 0) throw std::invalid_argument("nssb_batch_run: the batched form takes radius-0 filters");
+        if (it.cfg->kaiser_beta != 0.f)
+            throw std::invalid_argument("nssb_batch_run: a node with the Kaiser window renders per frame only");
         if (it.cfg->device_id != device_)
             throw std::invalid_argument("nssb_batch_run: node lives on another device than the batch");
         if (it.cfg->has_ref && !it.ref) throw std::invalid_argument("nssb_batch_run: ref frame missing");

@@ -3,9 +3,11 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <cstring>
+#include <vector>
 
 namespace nssb {
 
@@ -293,6 +295,72 @@ void Engine::stats(int enable_timing, int reset, nssb_kernel_stats* out) {
     timing_ = enable_timing != 0;
 }
 
+namespace {
+
+// Modified Bessel function of the first kind, order 0, by its power series
+// sum_k ((x/2)^k / k!)^2 (terms added until they fall below 1e-17 of the sum).
+double bessel_i0(double x) {
+    double term = 1.0, sum = 1.0;
+    int k = 1;
+    while (term > 1e-17 * sum) {
+        const double y = x / (2.0 * k);
+        term *= y * y;
+        sum += term;
+        ++k;
+    }
+    return sum;
+}
+
+// The separable n x n Kaiser window: w(i) = I0(beta sqrt(1 - r_i^2)) / I0(beta),
+// r_i = 2i/(n-1) - 1, and win(i, j) = w(i) w(j) rounded to float.
+std::vector<float> kaiser_window(int n, double beta) {
+    std::vector<double> w1(n, 1.0);
+    if (n > 1) {
+        for (int i = 0; i < n; ++i) {
+            const double r = 2.0 * i / (n - 1) - 1.0;
+            w1[i] = bessel_i0(beta * std::sqrt(std::max(0.0, 1.0 - r * r))) / bessel_i0(beta);
+        }
+    }
+    std::vector<float> w((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) w[(size_t)i * n + j] = (float)(w1[i] * w1[j]);
+    return w;
+}
+
+}  // namespace
+
+void Engine::set_window(float beta) {
+    if (!(beta >= 0.f) || !std::isfinite(beta))
+        throw std::invalid_argument("nss_cuda.BM3D: the Kaiser window's beta must be finite and non-negative");
+    if (beta > 0.f && cfg_.radius > 0)
+        throw std::invalid_argument("nss_cuda.BM3D: the Kaiser window applies to radius-0 filters");
+    std::lock_guard<std::mutex> lock(mu_);
+    std::vector<Slot*> held;  // every slot idle: no frame may be reading the windows
+    for (size_t i = 0; i < slots_.size(); ++i) held.push_back(lease(false));
+    struct Back {
+        Engine* e;
+        std::vector<Slot*>& h;
+        ~Back() {
+            for (Slot* s : h) e->give_back(s);
+        }
+    } back{this, held};
+    windows_.clear();  // the old tables stay allocated until the engine goes
+    if (beta > 0.f) {
+        for (int p = 0; p < cfg_.planes; ++p) {
+            for (const StageParams* sp : {&cfg_.final_stage[p], &cfg_.basic_stage[p]}) {
+                const int b = sp->block;
+                if (windows_.count(b)) continue;
+                const std::vector<float> w = kaiser_window(b, beta);
+                auto* d = static_cast<float*>(dev_alloc(w.size() * sizeof(float)));
+                allocations_.push_back(d);
+                NSSB_CUDA(cudaMemcpy(d, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+                windows_[b] = d;
+            }
+        }
+    }
+    cfg_.kaiser_beta = beta;
+}
+
 // One stage over the planes of a frame (radius 0), one launch per kernel and shape.
 void Engine::run_stage(Slot& s, StageItem* items, int n) {
     StagePlane planes[3];
@@ -301,6 +369,7 @@ void Engine::run_stage(Slot& s, StageItem* items, int n) {
         planes[i] = StagePlane{it.sp, it.src, it.sstride, it.ref, it.rstride, it.dst, it.dstride,
                                cfg_.plane_w[it.plane], cfg_.plane_h[it.plane], s.acc[it.plane], &s.scratch[it.plane],
                                it.shared_pos, it.shared_count};
+        if (!windows_.empty()) planes[i].win = windows_.at(it.sp->block);
     }
     Clock clock(this, &s);
     run_stage_planes(planes, n, s.stream, tunes_, clock, s.tables);

@@ -82,6 +82,11 @@ public:
     // Slots the engine renders radius-0 frames on (num_streams).
     int slots() const { return (int)slots_.size(); }
 
+    // Opt-in Kaiser aggregation window: every patch pixel is weighted by the
+    // separable Kaiser window of the block (beta > 0) on top of the group's
+    // flat weight; 0 restores the reference's flat weights. Radius 0 only.
+    void set_window(float beta);
+
 private:
     struct Plan;
     // The buffers and stream of one frame in flight -- the reference's slots
@@ -147,6 +152,7 @@ private:
     std::mutex mu_;                              // temporal frames, matcher changes
     LaunchTunes tunes_;
     std::unique_ptr<Clock> clock_;               // slot 0's accounting (the temporal drivers')
+    std::map<int, float*> windows_;              // block size -> its window (device), when windowed
     std::vector<void*> allocations_;
     struct PlanDeleter {
         void operator()(Plan* p) const;

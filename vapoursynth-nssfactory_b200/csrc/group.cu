@@ -222,10 +222,15 @@ __global__ void __launch_bounds__(128) group_kernel(GroupIO io, int W, int H, co
             const int32_t p = jp[g];
             const int s = js ? js[g] : 0;
             const int64_t off = (int64_t)(pos_y(p) + i) * io.acc_stride + pos_x(p) + j;
+            // opt-in window: the pixel's own weight, its den per pixel
+            const float ww = io.win ? __fmul_rn(weight, __ldg(io.win + e)) : weight;
             atomicAdd(reinterpret_cast<unsigned long long*>(io.num[s] + off),
-                      static_cast<unsigned long long>(to_fixed(__fmul_rn(weight, cube[idx]))));
+                      static_cast<unsigned long long>(to_fixed(__fmul_rn(ww, cube[idx]))));
+            if (io.win)
+                atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[s] + off),
+                          static_cast<unsigned long long>(to_fixed(ww)));
         }
-        for (int g = tid; g < k; g += blockDim.x) {
+        for (int g = tid; g < k && !io.win; g += blockDim.x) {
             const int32_t p = jp[g];
             const int s = js ? js[g] : 0;
             const int64_t off = (int64_t)pos_y(p) * io.acc_stride + pos_x(p);

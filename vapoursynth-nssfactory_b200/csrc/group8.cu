@@ -172,11 +172,13 @@ __device__ __forceinline__ void load_row8(const float* rowp, int px, bool vec, f
 __device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // One group on one warp. Acc(s) gives the (num, wsum, stride) of slot s,
-// Src(s, row, x) / Ref(s, row, x) the source rows.
+// Src(s, row, x) / Ref(s, row, x) the source rows. win: the opt-in 8x8
+// aggregation window or null; with it each pixel adds its own weight
+// w * win to num (times the value) and to its den in wsum.
 template <int G, bool WIENER, class SrcRow, class RefRow, class AddNum, class AddWeight>
 __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane, int k, int32_t p, int s,
                                              float sigma, bool vec, SrcRow src_row, RefRow ref_row,
-                                             AddNum add_num, AddWeight add_weight) {
+                                             AddNum add_num, AddWeight add_weight, const float* win) {
     using Sh = Shape<G>;
     const int g = lane / Sh::LP, q = lane % Sh::LP;
     const int px = pos_x(p), py = pos_y(p);
@@ -277,7 +279,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         }
         __syncwarp();
         if (g < k) {
-            if (q == 0) add_weight(s, px, py, __float2ll_rn(wscaled));
+            if (q == 0 && !win) add_weight(s, px, py, __float2ll_rn(wscaled));
 #pragma unroll
             for (int t = 0; t < Sh::RPL; ++t) {
                 const int c = q + Sh::LP * t;
@@ -285,8 +287,18 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 #pragma unroll
                 for (int i = 0; i < 8; ++i) v[i] = cube[g * Sh::S + Sh::at(i, c)];
                 idct8(v);
+                if (win) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) add_num(s, px + c, py + i, __float2ll_rn(__fmul_rn(wscaled, v[i])));
+                    for (int i = 0; i < 8; ++i) {
+                        const float ww = __fmul_rn(weight, __ldg(win + i * 8 + c));
+                        add_num(s, px + c, py + i, to_fixed(__fmul_rn(ww, v[i])));
+                        add_weight(s, px + c, py + i, to_fixed(ww));
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        add_num(s, px + c, py + i, __float2ll_rn(__fmul_rn(wscaled, v[i])));
+                }
             }
         }
     } else {
@@ -306,7 +318,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 #pragma unroll
             for (int j = 0; j < 8; ++j) cube[g * Sh::S + Sh::at(row, j)] = v[j];
         }
-        if (g < k && q == 0) add_weight(s, px, py, __float2ll_rn(wscaled));
+        if (g < k && q == 0 && !win) add_weight(s, px, py, __float2ll_rn(wscaled));
         __syncwarp();
 #pragma unroll
         for (int gg = 0; gg < G; ++gg) {
@@ -316,8 +328,14 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int i = 4 * h + (lane >> 3), j = lane & 7;
-                add_num(ss, pos_x(pp) + j, pos_y(pp) + i,
-                        __float2ll_rn(__fmul_rn(wscaled, cube[gg * Sh::S + Sh::at(i, j)])));
+                const float v = cube[gg * Sh::S + Sh::at(i, j)];
+                if (win) {
+                    const float ww = __fmul_rn(weight, __ldg(win + i * 8 + j));
+                    add_num(ss, pos_x(pp) + j, pos_y(pp) + i, to_fixed(__fmul_rn(ww, v)));
+                    add_weight(ss, pos_x(pp) + j, pos_y(pp) + i, to_fixed(ww));
+                } else {
+                    add_num(ss, pos_x(pp) + j, pos_y(pp) + i, __float2ll_rn(__fmul_rn(wscaled, v)));
+                }
             }
         }
     }
@@ -354,7 +372,8 @@ __global__ void __launch_bounds__(32 * NW) group8_kernel(GroupIO io, const int32
             [&](int sl, int x, int y, long long v) {
                 atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
                           (unsigned long long)v);
-            });
+            },
+            io.win);
     }
 }
 
@@ -409,7 +428,8 @@ __global__ void __launch_bounds__(32 * NW) group8_slots_batch_kernel(const __gri
                 [&](int sl, int x, int y, long long v) {
                     atomicAdd(reinterpret_cast<unsigned long long*>(io.wsum[sl] + (int64_t)y * io.acc_stride + x),
                               (unsigned long long)v);
-                });
+                },
+                io.win);
         }
         k = kn;
         s = sn;
@@ -460,7 +480,8 @@ __global__ void __launch_bounds__(32 * NW) group8_batch_kernel(const __grid_cons
                 [&](int, int x, int y, long long v) {
                     atomicAdd(reinterpret_cast<unsigned long long*>(P_.wsum + (int64_t)y * P_.acc_stride + x),
                               (unsigned long long)v);
-                });
+                },
+                P_.win);
         }
         k = kn;
         p = pn;

@@ -29,6 +29,9 @@ struct MatchPlane {
     // origin weights, cleared for the group filter that follows), or null
     long long* clear = nullptr;
     int64_t clear_words = 0;
+    // 8x8 matchers: the grid columns [rx_begin, rx_end) of references to
+    // match (rx_end 0: up to the last)
+    int rx_begin = 0, rx_end = 0;
 };
 struct MatchBatch {
     int n, step;
@@ -52,6 +55,12 @@ bool launch_match8_batch(MatchBatch& batch, int bm_range, int group, cudaStream_
                          const MatchTune* tune = nullptr);
 bool launch_match8(const float* plane, int64_t stride, int width, int height, int step, int bm_range, int group,
                    int32_t* pos, float* dist, int32_t* count, cudaStream_t stream);
+// The 8x8 direct matcher alone (every reference's 64 columns on its own lanes).
+bool launch_match8_direct(MatchBatch& batch, int bm_range, int group, cudaStream_t stream, const MatchTune* tune);
+// The column-reuse matcher for 8x8 blocks at steps 1-4 (match_col8.cu):
+// whether it takes the shape, and the launch (false when it does not).
+bool matchcol_takes(int step, int bm_range, int group);
+bool launch_matchcol_batch(MatchBatch& batch, int bm_range, int group, cudaStream_t stream);
 
 // Precision form of the 8x8 matcher (match_tc.cu): BF16 tensor-core distances,
 // exact FP32 re-rank; the same lists as launch_match8_batch. Counters (device
@@ -77,6 +86,10 @@ struct GroupPlane {
     float sigma;
     int W, H;   // plane size
     int cta0;   // first CTA of this plane
+    // opt-in aggregation window (block x block weights, device memory), or
+    // null: each pixel then adds w * win to num (times the value) and to a
+    // per-pixel den in wsum (finished with a 1 x 1 box)
+    const float* win = nullptr;
 };
 struct GroupBatch {
     int n, total_jobs;
@@ -147,6 +160,7 @@ struct GroupIO {
     long long* num[kMaxSlots];
     long long* wsum[kMaxSlots];
     int64_t acc_stride;           // element stride of num/wsum
+    const float* win = nullptr;   // opt-in aggregation window, as in GroupPlane
 };
 void launch_group_filter(const GroupIO& io, int width, int height, const int32_t* pos, const int32_t* slot,
                          const int32_t* count, int njobs, int block, int group, float sigma, bool wiener,

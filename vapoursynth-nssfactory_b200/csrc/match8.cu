@@ -75,14 +75,18 @@ struct TopK {
 
 // Groups of 32: the 31-entry list split over the two lanes of a reference
 // (half 0 the 16 smallest keys, half 1 the next 15), so a lane holds no more
-// registers than the 15-entry list. Both lanes offer every key: half 0 puts
-// it into its list when it beats that list's last entry, and what leaves
-// half 0's list (or the key) goes on to half 1's; both lanes then take the
-// overall worst from half 1, so they agree on every pass mask and run the
-// same insertions (the pair's shuffles use the pair's own lane mask).
+// registers than the 15-entry list. Every key of half 0's list is below every
+// key of half 1's, so a new key v enters as follows, both lanes running the
+// same instructions: half 0 inserts v (a no-op unless v beats its last key);
+// half 1 inserts max(v, half 0's last key) -- v itself, or the key half 0
+// lets go, which lands at half 1's front. Half 1's 16th slot is scratch.
+// Both lanes then take the overall worst (half 1's 15th key), so they agree
+// on every pass mask and run the same insertions (the pair's shuffles use
+// the pair's own lane mask).
 template <int K>
 struct SplitTopK {
     static constexpr int LO = (K + 1) / 2, HI = K - LO, kHeld = LO;
+    static_assert(HI <= LO, "half 1's list fits in half 0's length");
     uint64_t k[LO];
     uint64_t worst_;
     int half, lo_lane, hi_lane;
@@ -98,10 +102,8 @@ struct SplitTopK {
     }
     __device__ __forceinline__ void add(uint64_t v) {
         if (!(v < worst_)) return;  // the same decision in both lanes
-        uint64_t up = v;
-        if (half == 0) up = sorted_insert<LO>(k, v);
-        up = __shfl_sync(pair, up, lo_lane);  // what half 0 let go, in both lanes
-        if (half == 1) (void)sorted_insert<HI>(k, up);
+        const uint64_t lo_last = __shfl_sync(pair, k[LO - 1], lo_lane);
+        (void)sorted_insert<LO>(k, half == 0 || v > lo_last ? v : lo_last);
         worst_ = __shfl_sync(pair, k[HI - 1], hi_lane);
     }
     __device__ __forceinline__ uint64_t worst() const { return worst_; }
@@ -149,10 +151,11 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     }
     const MatchPlane& P_ = mb.p[pl];
     const int W = P_.W, H = P_.H, step = mb.step, nx = P_.nx;
+    const int rxe = P_.rx_end > 0 ? P_.rx_end : nx;  // grid columns [rx_begin, rxe)
     const int local = tile_id - P_.cta0;
-    const int chunks = (nx + kLanes - 1) / kLanes;
-    const int ry = local / chunks, rx0 = (local - ry * chunks) * kLanes;
-    const int rx1 = min(rx0 + kLanes, nx) - 1;
+    const int chunks = (rxe - P_.rx_begin + kLanes - 1) / kLanes;
+    const int ry = local / chunks, rx0 = P_.rx_begin + (local - ry * chunks) * kLanes;
+    const int rx1 = min(rx0 + kLanes, rxe) - 1;
     const int cy = grid_pos(ry, H, B, step);
     const int X0 = grid_pos(rx0, W, B, step) - R, Y0 = cy - R;
     const int TW = grid_pos(rx1, W, B, step) + R + B - X0;
@@ -183,8 +186,8 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     const int rg = warp & 1, part = warp >> 1, half = lane >> 4;
     const int l = rg * 16 + (lane & 15);
     const int rx = rx0 + l;
-    const bool active = rx < nx;
-    const int cx = grid_pos(min(rx, nx - 1), W, B, step);
+    const bool active = rx < rxe;
+    const int cx = grid_pos(min(rx, rxe - 1), W, B, step);
     // the window's own range Rr <= R: a kernel built for range R serves any
     // smaller range, its rows and columns beyond Rr masked or skipped
     const int Rr = mb.range;
@@ -331,7 +334,7 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
         p.nx = grid_count(p.W, 8, mb.step);
         p.ny = grid_count(p.H, 8, mb.step);
         p.cta0 = ctas;
-        ctas += ceil_div(p.nx, kLanes) * p.ny;
+        ctas += ceil_div((p.rx_end > 0 ? p.rx_end : p.nx) - p.rx_begin, kLanes) * p.ny;
     }
     mb.total_ctas = ctas;
     mb.queue = nullptr;
@@ -386,6 +389,12 @@ bool launch_r(MatchBatch& mb, int group, const MatchTune& tune, cudaStream_t str
 }  // namespace
 
 bool launch_match8_batch(MatchBatch& mb, int bm_range, int group, cudaStream_t stream, const MatchTune* tune) {
+    // dense steps: the column-reuse matcher where it takes the shape
+    if (matchcol_takes(mb.step, bm_range, group) && launch_matchcol_batch(mb, bm_range, group, stream)) return true;
+    return launch_match8_direct(mb, bm_range, group, stream, tune);
+}
+
+bool launch_match8_direct(MatchBatch& mb, int bm_range, int group, cudaStream_t stream, const MatchTune* tune) {
     if (mb.step < 1 || mb.step > 8 || mb.n < 1 || mb.n > kMaxBatchPlanes) return false;
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8) return false;

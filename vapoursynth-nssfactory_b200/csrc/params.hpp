@@ -51,6 +51,9 @@ struct Bm3dConfig {
     int64_t memory_limit_mb = 0; // 0 = none
     int device_id = 0;
     int num_streams = 1;
+    // Opt-in Kaiser aggregation window (nssb_bm3d_set_window; not a filter
+    // argument): 0 = the reference's flat per-group weights.
+    float kaiser_beta = 0.f;
 };
 
 // Throws ArgumentError with the filter's message.

@@ -20,7 +20,7 @@ __global__ void clear_wsum_kernel(const __grid_constant__ GroupBatch gb) {
 bool same_shape(const StagePlane& a, const StagePlane& b) {
     const StageParams &x = *a.sp, &y = *b.sp;
     return x.block == y.block && x.group == y.group && x.step == y.step && x.bm_range == y.bm_range &&
-           (a.ref != nullptr) == (b.ref != nullptr);
+           (a.ref != nullptr) == (b.ref != nullptr) && a.win == b.win;
 }
 
 // One launch set over planes[set[0..ns)] (same shape, ns <= kMaxBatchPlanes).
@@ -84,7 +84,7 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
         gb.p[gb.n++] = GroupPlane{it.src, it.ref, it.sstride, it.rstride, it.acc.num, it.acc.wsum, it.acc.pitch,
                                   it.shared_pos ? it.shared_pos : it.sc->pos,
                                   it.shared_count ? it.shared_count : it.sc->count, gb.total_jobs, jobs,
-                                  it.sp->sigma, it.w, it.h, 0};
+                                  it.sp->sigma, it.w, it.h, 0, it.win};
         gb.total_jobs += jobs;
     }
     if (!(cleared && fuse_clear)) {
@@ -112,6 +112,7 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
             io.num[0] = g.num;
             io.wsum[0] = g.wsum;
             io.acc_stride = g.acc_stride;
+            io.win = g.win;
             clock.begin(StageClock::kGroup);
             launch_group_filter(io, it.w, it.h, g.pos, nullptr, g.count, g.njobs, sp.block, sp.group, g.sigma,
                                 wiener, it.sc->cube, it.sc->cube_floats, stream);
@@ -121,7 +122,7 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
     // finish (clears num)
     FinishBatch& fb = t.finish;
     fb.n = 0;
-    fb.block = sp.block;
+    fb.block = first.win ? 1 : sp.block;  // windowed: wsum already holds each pixel's den
     fb.total_ctas = 0;
     for (int q = 0; q < ns; ++q) {
         const StagePlane& it = planes[set[q]];

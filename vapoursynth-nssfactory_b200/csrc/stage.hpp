@@ -47,6 +47,7 @@ struct StagePlane {
     const StageScratch* sc;
     const int32_t* shared_pos;    // CBM3D: groups matched on another plane of the same stage
     const int32_t* shared_count;
+    const float* win = nullptr;   // opt-in aggregation window (block x block, device), or null
 };
 
 // Launch shapes of the specialised kernels (results do not depend on them).
