@@ -318,12 +318,7 @@ def our_arm(args):
     flops_per_launch = stats.match_flops / max(1, launches)
     achieved = flops_per_launch / (per_launch_ms / 1e3) / 1e12 if per_launch_ms > 0 else 0.0
     fp32_peak = FP32_LANES * 2 * sm_max * 1e6 / 1e12
-    traffic = None
-    tfile = ROOT / "profiles" / "match8_group8_finish_two_stage_yuv420_1080p.md"
-    if tfile.exists():
-        for line in tfile.read_text().splitlines():
-            if line.strip().startswith("bytes_per_launch_c2="):
-                traffic = float(line.split("=", 1)[1])
+    traffic, traffic_note = match8_traffic()
     out = {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -341,6 +336,8 @@ def our_arm(args):
                 "d2h_bytes_per_step": nf * PLANE_BYTES},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                     "traffic_note": traffic_note,
+                     "frac_of_sub_fma_ceiling": achieved / (0.75 * fp32_peak) if fp32_peak else None,
                      "kernel": "match8_kernel (exact FP32 SSD + top-k; its tiles also zero the stage's origin weights)",
                      "peak_kind": f"derived: 148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz ({peak_kind} max clock)",
                      "avg_launch_ms": per_launch_ms, "flops_per_launch": flops_per_launch},
@@ -520,6 +517,27 @@ def c2_parity_leg(frames, gpu_out, threads, n=16):
     return {"frames": k, "psnr_vs_cpu_db_min": float(min(ps)), "psnr_vs_cpu_db_mean": float(np.mean(ps)),
             "cpu_s": time.perf_counter() - t0, "note": "full 1920x1080 YUV420 frames, batched form vs the CPU "
             "restatement (oracle/), PSNR pooled over the three planes per frame"}
+
+
+def match8_traffic():
+    """DRAM bytes (read + write) of one matcher launch on the headline frame,
+    from the committed ncu summary -- only while it was captured from the
+    current matcher source (its SHA-256 is recorded beside the number)."""
+    import hashlib
+
+    tfile = ROOT / "profiles" / "match8_traffic_two_stage_yuv420_1080p.md"
+    src = ROOT / "vapoursynth-nssfactory_b200" / "csrc" / "match8.cu"
+    if not tfile.exists():
+        return None, "no ncu summary"
+    fields = {}
+    for line in tfile.read_text().splitlines():
+        if "=" in line and line.strip().split("=", 1)[0] in ("bytes_per_launch_c2", "match8_cu_sha256"):
+            k, v = line.strip().split("=", 1)
+            fields[k] = v
+    have = hashlib.sha256(src.read_bytes()).hexdigest()
+    if fields.get("match8_cu_sha256") != have:
+        return None, "stale: the ncu summary was captured from another match8.cu"
+    return float(fields["bytes_per_launch_c2"]), "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"
 
 
 def accuracy_leg(nssb, frame, dev):

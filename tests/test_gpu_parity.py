@@ -67,7 +67,9 @@ SHAPES = [(8, 8, 8, 9), (8, 4, 16, 9), (4, 4, 8, 6), (8, 8, 32, 5), (16, 8, 16, 
           # steps 1-4 on the column-reuse matcher (the last grid column clamped at W = 61
           # for steps 2-4 goes to the direct one)
           (8, 1, 8, 9), (8, 2, 16, 16), (8, 3, 8, 25), (8, 4, 8, 31), (8, 3, 4, 12), (8, 1, 16, 19),
-          (8, 2, 4, 10), (8, 4, 32, 19)]
+          (8, 2, 4, 10), (8, 4, 32, 19),
+          # ranges 32-64 on the 8x8 matcher, in bands of 63 x 63 candidates
+          (8, 8, 8, 40), (8, 8, 16, 64), (8, 6, 32, 45), (8, 3, 8, 33)]
 
 
 @pytest.mark.parametrize("block,step,group,rng_", SHAPES)
@@ -88,7 +90,7 @@ def test_match_spatial_exact(nssb, oracle, synth, dev, block, step, group, rng_)
 
 @pytest.mark.parametrize("rng_,group,step", [(16, 8, 8), (25, 16, 8), (20, 8, 8), (30, 4, 8), (11, 8, 8), (19, 32, 8),
                                              (19, 16, 8), (31, 32, 8), (19, 16, 3), (19, 32, 3), (9, 8, 4),
-                                             (12, 16, 2)])
+                                             (12, 16, 2), (40, 8, 8), (64, 16, 8), (33, 32, 4)])
 def test_match_large_window_whole(nssb, oracle, synth, dev, rng_, group, step):
     # windows well inside a larger plane (most references see the whole window)
     noisy, _ = synth.gray_frame(17, 256, 160, sigma=10)

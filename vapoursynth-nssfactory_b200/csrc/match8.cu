@@ -1,7 +1,8 @@
 // Exact FP32 block matching for 8x8 blocks (sm_100a): the default BM3D shape
-// (bm_range 9), and every range from 4 to 31 (kernels built for 4-9, 12,
-// 15, 16, 19, 25 and 31; a range between two runs on the larger one), groups
-// of 2, 4, 8, 16 and 32.
+// (bm_range 9), and every range from 4 to 64 (kernels built for 4-9, 12,
+// 15, 16, 19, 25 and 31; a range between two runs on the larger one, a range
+// beyond 31 on the 31 kernel in bands of 63 x 63 candidates), groups of 2,
+// 4, 8, 16 and 32.
 //
 // Same contract as match.cu (the reference's matcher.hpp:27-283 ordering,
 // keys dist << 32 | y << 16 | x, and this build's SSD order: one FMA chain per
@@ -157,9 +158,39 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     const int ry = local / chunks, rx0 = P_.rx_begin + (local - ry * chunks) * kLanes;
     const int rx1 = min(rx0 + kLanes, rxe) - 1;
     const int cy = grid_pos(ry, H, B, step);
-    const int X0 = grid_pos(rx0, W, B, step) - R, Y0 = cy - R;
-    const int TW = grid_pos(rx1, W, B, step) + R + B - X0;
+    const int xr0 = grid_pos(rx0, W, B, step);
+    const int TW = grid_pos(rx1, W, B, step) - xr0 + NC + B - 1;  // tile columns
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rg = warp & 1, part = warp >> 1, half = lane >> 4;
+    const int l = rg * 16 + (lane & 15);
+    const int rx = rx0 + l;
+    const bool active = rx < rxe;
+    const int cx = grid_pos(min(rx, rxe - 1), W, B, step);
+    // The window's own range Rr: up to R, a kernel built for range R serves
+    // it in one pass (rows and columns beyond Rr masked or skipped); beyond R
+    // (ranges 32-64 on the R = 31 kernel) the window is swept in bands of
+    // NC x NC candidates, the tile reloaded per band and the lists carried
+    // in registers from band to band.
+    const int Rr = mb.range;
+    const bool banded = Rr > R;
+    const int nb = banded ? (2 * Rr + NC) / NC : 1;  // bands per axis: ceil((2 Rr + 1) / NC)
+    const int left = max(cx - Rr, 0), right = min(cx + Rr, W - B);
+    const int tc0 = cx - xr0 + HB * half;  // tile column of this half's first block column at band column 0
+
+    float2 ref[B][2];
+    using List = typename std::conditional<(K > 15), SplitTopK<K>, TopK<K>>::type;
+    List topk;
+    topk.init(lane);
+    // finished distances of the current column, one slot per candidate row:
+    // an emit stores its sum and marks a bit when it may enter the list; the
+    // insertions run after the column, once per marked candidate
+    float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
+    const float2 neg1 = make_float2(-1.f, -1.f);
+    for (int band = 0; band < nb * nb; ++band) {
+    // candidate (band column d, band row k) is (cx + ox + d, cy + oy + k)
+    const int ox = banded ? -Rr + (band % nb) * NC : -R, oy = banded ? -Rr + (band / nb) * NC : -R;
+    const int X0 = xr0 + ox, Y0 = cy + oy;
+    if (band > 0) __syncthreads();  // every warp is done with the previous band's tile
     for (int r = warp; r < TR; r += 2 * P) {
         const int gy = Y0 + r;
         const bool yok = gy >= 0 && gy < H;
@@ -173,7 +204,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     }
     // this tile's share of the plane's words to clear, stored while the
     // window rows are in flight (an even count per tile: 16-byte stores)
-    if (P_.clear) {
+    if (band == 0 && P_.clear) {
         const int tiles = chunks * P_.ny;
         const int64_t per = ((P_.clear_words + tiles - 1) / tiles + 1) & ~int64_t(1);
         const int64_t a = (int64_t)local * per, b = min(P_.clear_words, a + per);
@@ -182,45 +213,34 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     }
     cp_async_wait_all();
     __syncthreads();
-
-    const int rg = warp & 1, part = warp >> 1, half = lane >> 4;
-    const int l = rg * 16 + (lane & 15);
-    const int rx = rx0 + l;
-    const bool active = rx < rxe;
-    const int cx = grid_pos(min(rx, rxe - 1), W, B, step);
-    // the window's own range Rr <= R: a kernel built for range R serves any
-    // smaller range, its rows and columns beyond Rr masked or skipped
-    const int Rr = mb.range;
-    const int left = max(cx - Rr, 0), right = min(cx + Rr, W - B);
-    const int kmin = max(cy - Rr, 0) - (cy - R), kmax = min(cy + Rr, H - B) - (cy - R);
-    const int tc0 = cx - R - X0 + HB * half;  // tile column of this half's first block column at dx = -R
-
-    // this half's 8x4 reference block as column pairs (c, c+1) of each row
-    float2 ref[B][2];
+    if (band == 0) {
+        // this half's 8x4 reference block as column pairs (c, c+1) of each
+        // row: from the tile (rows R.. hold the block), or from the plane when banded
 #pragma unroll
-    for (int i = 0; i < B; ++i)
+        for (int i = 0; i < B; ++i)
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-            ref[i][h] = make_float2(tile[(R + i) * kPitch + swz(tc0 + R + 2 * h)],
-                                    tile[(R + i) * kPitch + swz(tc0 + R + 2 * h + 1)]);
-
-    using List = typename std::conditional<(K > 15), SplitTopK<K>, TopK<K>>::type;
-    List topk;
-    topk.init(lane);
-    // finished distances of the current column, one slot per candidate row:
-    // an emit stores its sum and marks a bit when it may enter the list; the
-    // insertions run after the column, once per marked candidate
-    float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
-    const Mask rows_ok = ((Mask(1) << (kmax + 1)) - 1) & ~((Mask(1) << kmin) - 1);
-    const float2 neg1 = make_float2(-1.f, -1.f);
-    // this part's columns, walked outwards from the window centre so the
-    // closest candidates (usually the best) fill the list first
-    const int cpw = (2 * Rr + P) / P;  // ceil((2 Rr + 1) / P)
-    const int d0 = (R - Rr) + part * cpw, d1 = min(R + Rr + 1, d0 + cpw);
-    const bool down = d1 - 1 <= R;
+            for (int h = 0; h < 2; ++h) {
+                if (banded) {
+                    const float* rp = P_.src + (int64_t)(cy + i) * P_.stride + cx + HB * half + 2 * h;
+                    ref[i][h] = make_float2(__ldg(rp), __ldg(rp + 1));
+                } else {
+                    ref[i][h] = make_float2(tile[(R + i) * kPitch + swz(tc0 + R + 2 * h)],
+                                            tile[(R + i) * kPitch + swz(tc0 + R + 2 * h + 1)]);
+                }
+            }
+    }
+    // the band's candidate rows inside the reference's clamped window
+    const int klo = max(max(cy - Rr, 0) - (cy + oy), 0), khi = min(min(cy + Rr, H - B) - (cy + oy), NC - 1);
+    const Mask rows_ok = klo > khi ? Mask(0) : ((Mask(1) << (khi + 1)) - 1) & ~((Mask(1) << klo) - 1);
+    // this part's columns: unbanded, walked outwards from the window centre
+    // so the closest candidates (usually the best) fill the list first
+    const int ncols = banded ? min(NC, Rr - ox + 1) : 2 * Rr + 1;
+    const int cpw = (ncols + P - 1) / P;
+    const int d0 = (banded ? 0 : R - Rr) + part * cpw, d1 = min((banded ? 0 : R - Rr) + ncols, d0 + cpw);
+    const bool down = !banded && d1 - 1 <= R;
     for (int m = 0; m < d1 - d0; ++m) {
         const int dxi = down ? d1 - 1 - m : d0 + m;
-        const int x = cx - R + dxi;
+        const int x = cx + ox + dxi;
         const bool xok = x >= left && x <= right;
         Mask pass = 0;
         // a candidate may enter unless it is farther than the current worst
@@ -260,13 +280,14 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
             }
         }
         pass &= xok ? rows_ok : Mask(0);
-        if (dxi == R) pass &= ~(Mask(1) << R);
+        if (dxi == -ox && -oy >= 0 && -oy < NC) pass &= ~(Mask(1) << -oy);  // the reference itself
         while (pass) {
             const int kd = first_bit(pass);
             pass &= pass - 1;
-            topk.add(key_of(stash[kd * (64 * P)], x, cy - R + kd));
+            topk.add(key_of(stash[kd * (64 * P)], x, cy + oy + kd));
         }
     }
+    }  // bands
     // merge the P partial lists of each reference (exact: keys are a total order)
     if constexpr (P > 1) {
         __syncthreads();
@@ -419,7 +440,7 @@ bool launch_match8_direct(MatchBatch& mb, int bm_range, int group, cudaStream_t 
     if (bm_range <= 16) return launch_r<16>(mb, group, t, stream);
     if (bm_range <= 19) return launch_r<19>(mb, group, t, stream);
     if (bm_range <= 25) return launch_r<25>(mb, group, t, stream);
-    if (bm_range <= 31) return launch_r<31>(mb, group, t, stream);
+    if (bm_range <= 64) return launch_r<31>(mb, group, t, stream);  // beyond 31: in bands
     return false;
 }
 
