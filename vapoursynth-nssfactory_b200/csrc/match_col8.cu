@@ -24,7 +24,11 @@
 //     from the next h lanes' column sums by shuffles, so each column sum is
 //     formed once for the ceil(8/S) references that use it;
 //   - one register top-k per reference (its lane); the P partial lists merge
-//     in shared memory.
+//     in shared memory. While they run, each part publishes its list's last
+//     key after every window column and filters its candidates against the
+//     smallest of the parts' last keys: a candidate farther than some part's
+//     K-th is beaten by K others and cannot make the merged list, so the
+//     parts together insert about as often as one list would.
 // The last grid column is clamped to W-8 when the step does not divide
 // W-8; that reference's columns are off the lanes' grid, so the 8x8 direct
 // matcher (match8.cu) takes that one grid column.
@@ -106,8 +110,13 @@ __device__ __forceinline__ float assemble(const float* c) {
     }
 }
 
+// Resident CTAs per SM the launch bounds ask for: 16 warps (128 registers)
+// up to groups of 16, 12 warps for groups of 32.
+template <int K, int P>
+__host__ __device__ constexpr int matchcol_min_blocks() { return (K <= 15 ? 16 : 12) / P; }
+
 template <int S, int R, int K, int P>
-__global__ void __launch_bounds__(32 * P) matchcol_kernel(const __grid_constant__ MatchBatch mb) {
+__global__ void __launch_bounds__(32 * P, matchcol_min_blocks<K, P>()) matchcol_kernel(const __grid_constant__ MatchBatch mb) {
     constexpr int B = 8, NC = 2 * R + 1, TR = col_rows<R>(), kPitch = col_pitch<S, R>();
     constexpr int NREF = refs_per_cta<S>();
     constexpr int S2 = S / 2;  // packed column pairs
@@ -153,6 +162,9 @@ __global__ void __launch_bounds__(32 * P) matchcol_kernel(const __grid_constant_
         for (int64_t i = a + 2 * threadIdx.x; i + 1 < b; i += 2 * (int64_t)blockDim.x)
             *reinterpret_cast<longlong2*>(P_.clear + i) = make_longlong2(0, 0);
     }
+    // each part's current last key per reference, for the shared filter
+    volatile uint64_t* part_last = reinterpret_cast<volatile uint64_t*>(tile + TR * kPitch + NC * 32 * P);
+    part_last[warp * 32 + lane] = ~0ull;
     cp_async_wait_all();
     __syncthreads();
 
@@ -188,7 +200,12 @@ __global__ void __launch_bounds__(32 * P) matchcol_kernel(const __grid_constant_
         const int x = cx - R + dxi;
         const bool xok = is_ref && x >= left && x <= right;
         Mask pass = 0;
-        const float worst = __uint_as_float(uint32_t(topk.k[K - 1] >> 32));
+        // the tightest last key of the P parts (a stale one is only looser)
+        uint64_t last = topk.k[K - 1];
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (q != part) last = min(last, (uint64_t)part_last[q * 32 + lane]);
+        const float worst = __uint_as_float(uint32_t(last >> 32));
         int col[S];
 #pragma unroll
         for (int j = 0; j < S; ++j) col[j] = tcol<S>(c0 + dxi + j);
@@ -247,6 +264,7 @@ __global__ void __launch_bounds__(32 * P) matchcol_kernel(const __grid_constant_
             pass &= pass - 1;
             topk.add(col_key(stash[kd * (32 * P)], x, cy - R + kd));
         }
+        part_last[part * 32 + lane] = topk.k[K - 1];
     }
     if constexpr (P > 1) {
         __syncthreads();
@@ -298,7 +316,8 @@ void launch_srk(MatchBatch& mb, cudaStream_t stream) {
     if (ctas == 0) return;
     static_assert(2 * R + 1 <= 64, "a column's candidates must fit the row mask");
     const size_t smem =
-        std::max((size_t)(col_pitch<S, R>() * col_rows<R>() + (2 * R + 1) * 32 * kParts) * sizeof(float),
+        std::max((size_t)(col_pitch<S, R>() * col_rows<R>() + (2 * R + 1) * 32 * kParts) * sizeof(float) +
+                     (size_t)kParts * 32 * sizeof(uint64_t),
                  (size_t)kParts * K * 32 * sizeof(uint64_t));
     auto kern = matchcol_kernel<S, R, K, kParts>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
