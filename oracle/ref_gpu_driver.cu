@@ -36,7 +36,7 @@ thread_local std::string g_error;
 struct Ctx {
     int max_w = 0, max_h = 0;
     nss_cuda::DeviceBuffer matches, counts, fixed_num, fixed_den, rows, values, patches, ref_cube, fnum, fden, ptrs,
-        tensor;
+        tensor, frames;
     std::unique_ptr<nss_cuda::OrderedAggregator> agg;
     size_t cap_entries = 0;
 };
@@ -212,6 +212,50 @@ int refgpu_stage(void* ctx, const float* src, const float* ref, float* dst, int 
                        stream, false);
             aggregate_finish(c.fnum.as<float>(), c.fden.as<float>(), src, w, h, w, dst, stream);
         }
+    });
+}
+
+// Temporal (predictive) matching of every reference of the centre slot t0
+// over ntemp frames (host array of device plane pointers, dense, pitch =
+// width), valid slots [valid_begin, valid_end): the reference's choice of
+// filter_center for radius > 0 (group_driver.cpp:800-810): its square
+// matcher's centre frame where that takes the shape, else the window
+// matcher's, else the lane kernels throughout.
+int refgpu_match_temporal(void* ctx, const float* const* planes, int ntemp, int t0, int valid_begin, int valid_end,
+                          int w, int h, int block, int step, int range, int group, int ps_num, int ps_range,
+                          void* matches, int* counts, void* stream_) {
+    return guarded([&] {
+        using namespace nss_cuda;
+        Ctx& c = *static_cast<Ctx*>(ctx);
+        auto stream = static_cast<cudaStream_t>(stream_);
+        if (ntemp < 1 || ntemp > 33) throw std::invalid_argument("refgpu_match_temporal: 1 to 33 frames");
+        reserve(c, w, h, block, step, group, false);
+        ensure(c.frames, 33 * sizeof(float*));
+        check(cudaMemcpyAsync(c.frames.get(), planes, ntemp * sizeof(float*), cudaMemcpyHostToDevice, stream),
+              "frame table");
+        check(cudaStreamSynchronize(stream), "frame table");  // pageable source: the copy is done before it changes
+        const RasterGrid grid = make_raster_grid(w, h, block, step);
+        const MatchGeometry g = geometry_of(w, h, block, range, group);
+        TemporalWindow win{};
+        win.frames = c.frames.as<const float*>();
+        win.ntemp = ntemp;
+        win.t0 = t0;
+        win.radius = t0;
+        win.valid_begin = valid_begin;
+        win.valid_end = valid_end;
+        win.ps_num = ps_num;
+        win.ps_range = ps_range;
+        const int n = grid.count();
+        auto* out = c.matches.as<DeviceMatch>();
+        auto* cnt = c.counts.as<int>();
+        if (!predictive_match_square(g, win, grid, 0, n, out, cnt, stream) &&
+            !predictive_match_window(g, win, grid, 0, n, out, cnt, stream))
+            predictive_match(g, win, grid, 0, n, out, cnt, stream);
+        check(cudaMemcpyAsync(matches, out, (size_t)n * group * sizeof(DeviceMatch), cudaMemcpyDeviceToDevice,
+                              stream),
+              "copy matches");
+        check(cudaMemcpyAsync(counts, cnt, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, stream),
+              "copy counts");
     });
 }
 

@@ -42,6 +42,7 @@ def lib():
         L.refgpu_match.argtypes = [vp, vp] + [C.c_int] * 6 + [vp, vp, vp]
         L.refgpu_stage.argtypes = [vp, vp, vp, vp] + [C.c_int] * 6 + [C.c_float, vp]
         L.refgpu_matcher_kind.argtypes = [C.c_int] * 6
+        L.refgpu_match_temporal.argtypes = [vp, C.POINTER(vp)] + [C.c_int] * 12 + [vp, vp, vp]
         _lib = L
     return _lib
 
@@ -84,6 +85,17 @@ class RefGpu:
         step = min(8, block) if step is None else step
         _check(lib().refgpu_match(self._h, plane_ptr, width, height, block, step, bm_range, group, matches_ptr,
                                   counts_ptr, stream))
+
+
+def match_temporal(ctx: "RefGpu", plane_ptrs, t0: int, valid_begin: int, valid_end: int, width: int, height: int,
+                   block=8, step=8, bm_range=9, group=8, ps_num=2, ps_range=4, matches_ptr: int = 0,
+                   counts_ptr: int = 0, stream: int | None = None) -> None:
+    """The reference's predictive matching of the centre slot t0 over the
+    frames (device pointers of dense planes): DeviceMatch records and counts."""
+    arr = (C.c_void_p * len(plane_ptrs))(*plane_ptrs)
+    _check(lib().refgpu_match_temporal(ctx._h, arr, len(plane_ptrs), t0, valid_begin, valid_end, width, height,
+                                       block, step, bm_range, group, ps_num, ps_range, matches_ptr, counts_ptr,
+                                       stream))
 
 
 def matcher_kind(width, height, block=8, step=8, bm_range=9, group=8) -> str:

@@ -202,3 +202,49 @@ def test_c2_1080p_yuv420_two_stage_vs_reference_kernels(nssb, refgpu, ctx, dev, 
     p = psnr(ours, theirs)
     print(f"C2 1080p YUV420 two-stage: {p:.1f} dB against the reference kernels")
     assert p >= MIN_PSNR
+
+
+@pytest.mark.parametrize("radius,group,rng_,ps_num,ps_range", [(2, 8, 9, 2, 4), (1, 16, 9, 2, 4), (2, 4, 7, 1, 4),
+                                                               (1, 8, 5, 3, 3)])
+def test_temporal_match_lists_vs_reference_kernels(nssb, refgpu, ctx, dev, synth, radius, group, rng_, ps_num,
+                                                   ps_range):
+    """Predictive temporal matching of the centre frame over 2r+1 frames of a
+    panning sequence: this build's lists against the reference's own
+    predictive kernels (square / window / lane, its filter_center choice)."""
+    import ctypes as C
+
+    ntemp = 2 * radius + 1
+    w, h = 480, 272
+    frames = [f[0] for f in synth.panning_clip(40 + radius, w, h, frames=ntemp, sigma=10.0, yuv420=False)]
+    d = [torch.from_numpy(np.ascontiguousarray(f)).to(dev) for f in frames]
+    step = 8
+    n = grid(w, 8, step) * grid(h, 8, step)
+    pos = torch.full((n, group), -1, dtype=torch.int32, device=dev)
+    slot = torch.full((n, group), -1, dtype=torch.int32, device=dev)
+    dist = torch.zeros((n, group), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(n, dtype=torch.int32, device=dev)
+    ptrs = (C.c_void_p * ntemp)(*[t.data_ptr() for t in d])
+    strides = (C.c_int64 * ntemp)(*([w] * ntemp))
+    nssb.check(nssb.lib().nssb_match_temporal(ptrs, strides, ntemp, radius, 0, ntemp, w, h, 8, step, rng_, group,
+                                              ps_num, ps_range, pos.data_ptr(), slot.data_ptr(), dist.data_ptr(),
+                                              cnt.data_ptr(), None))
+    rec = torch.zeros((n, group, 4), dtype=torch.int32, device=dev)
+    rcnt = torch.zeros(n, dtype=torch.int32, device=dev)
+    refgpu.match_temporal(ctx, [t.data_ptr() for t in d], radius, 0, ntemp, w, h, 8, step, rng_, group, ps_num,
+                          ps_range, rec.data_ptr(), rcnt.data_ptr())
+    torch.cuda.synchronize()
+    r = rec.cpu().numpy()
+    theirs_pos = (r[..., 1] << 16) | r[..., 0]
+    theirs_slot = r[..., 2]
+    theirs_dist = r[..., 3].copy().view(np.float32)
+    ours_pos, ours_slot, ours_dist, ours_cnt = pos.cpu().numpy(), slot.cpu().numpy(), dist.cpu().numpy(), cnt.cpu().numpy()
+    assert np.array_equal(ours_cnt, rcnt.cpu().numpy())
+    valid = np.arange(group)[None, :] < ours_cnt[:, None]
+    differ = valid & ((ours_pos != theirs_pos) | (ours_slot != theirs_slot))
+    assert np.all(refgpu.near_tie(ours_dist[differ], theirs_dist[differ])), "a temporal match differs beyond a near tie"
+    same = valid & ~differ
+    assert np.all(refgpu.near_tie(ours_dist[same], theirs_dist[same]))
+    flips = int(np.any(differ, axis=1).sum())
+    print(f"temporal radius {radius} group {group} range {rng_} ps {ps_num}/{ps_range}: {flips} of {n} "
+          f"references with a near-tie flip")
+    assert flips <= max(2, n // 100)

@@ -133,8 +133,9 @@ __device__ __forceinline__ int first_bit(uint64_t m) { return __ffsll((long long
 template <int K, int P>
 __host__ __device__ constexpr int match8_min_blocks() { return (K <= 7 ? 16 : 12) / (2 * P) > 0 ? (K <= 7 ? 16 : 12) / (2 * P) : 1; }
 
-// One tile: 32 consecutive references of one grid row of one plane.
-template <int R, int K, int P>
+// One tile: 32 consecutive references of one grid row of one plane. BANDED:
+// the window's range exceeds R and is swept in bands (see below).
+template <int R, int K, int P, bool BANDED>
 __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, float* tile) {
     constexpr int B = 8, HB = 4;
     constexpr int NC = 2 * R + 1;            // candidates per window column
@@ -172,7 +173,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     // NC x NC candidates, the tile reloaded per band and the lists carried
     // in registers from band to band.
     const int Rr = mb.range;
-    const bool banded = Rr > R;
+    constexpr bool banded = BANDED;
     const int nb = banded ? (2 * Rr + NC) / NC : 1;  // bands per axis: ceil((2 Rr + 1) / NC)
     const int left = max(cx - Rr, 0), right = min(cx + Rr, W - B);
     const int tc0 = cx - xr0 + HB * half;  // tile column of this half's first block column at band column 0
@@ -331,14 +332,14 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
 // Grid form: CTA b takes tile b. Persistent form (mb.queue set): a CTA takes
 // tile blockIdx.x, then keeps taking the next untaken tile from the device
 // counter until none is left; the counter is zero at launch.
-template <int R, int K, int P>
+template <int R, int K, int P, bool BANDED>
 __global__ void __launch_bounds__(64 * P, match8_min_blocks<K, P>())
     match8_kernel(const __grid_constant__ MatchBatch mb) {
     extern __shared__ float tile[];
     __shared__ int next_tile;
     int t = blockIdx.x;
     while (t < mb.total_ctas) {
-        match8_tile<R, K, P>(mb, t, tile);
+        match8_tile<R, K, P, BANDED>(mb, t, tile);
         if (mb.queue == nullptr) break;
         __syncthreads();  // the tile buffer is free again
         if (threadIdx.x == 0) next_tile = atomicAdd(mb.queue, 1) + (int)gridDim.x;
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(64 * P, match8_min_blocks<K, P>())
     }
 }
 
-template <int R, int K, int P>
+template <int R, int K, int P, bool BANDED = false>
 void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
     int ctas = 0;
     for (int i = 0; i < mb.n; ++i) {
@@ -363,7 +364,7 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
     static_assert(2 * R + 1 <= 64, "a column's candidates must fit the row mask");
     const size_t smem = std::max((size_t)(tile_pitch<R>() * tile_rows<R>() + (2 * R + 1) * 64 * P) * sizeof(float),
                                  (size_t)P * K * kLanes * sizeof(uint64_t));
-    auto kern = match8_kernel<R, K, P>;
+    auto kern = match8_kernel<R, K, P, BANDED>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = ctas;
     if (tune.persistent && tune.queue) {
@@ -384,6 +385,10 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
 
 template <int R, int K>
 void launch_rk(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
+    if (mb.range > R) {  // ranges 32-64 on the 31 kernel, in bands
+        if constexpr (R == 31) launch_rkp<R, K, 2, true>(mb, tune, stream);
+        return;
+    }
     if constexpr (R == 9) {  // the default range: every column split the tuner may pick
         switch (tune.parts) {
             case 1: launch_rkp<R, K, 1>(mb, tune, stream); break;
