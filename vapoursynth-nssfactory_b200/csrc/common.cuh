@@ -1,6 +1,8 @@
 // Shared device/host helpers of the sm_100a BM3D library.
 #pragma once
 
+#include <type_traits>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -63,6 +65,22 @@ __device__ __forceinline__ float column_tree(const float* c) {
         return __fadd_rn(column_tree<N / 2>(c), column_tree<N - N / 2>(c + N / 2));
     }
 }
+
+#ifdef __CUDACC__
+// Compile-time integers and an unrolled loop over them (the matchers' row
+// schedules: accumulator slots stay register names).
+template <int N>
+using IC = std::integral_constant<int, N>;
+template <int N>
+__device__ __forceinline__ IC<N> ic() { return {}; }
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (B < E) {
+        f(IC<B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+#endif
 
 // Asynchronous 4-byte global -> shared copy (LDGSTS): a tile fill issues
 // all its copies without waiting on any, then waits once. bytes = 0 writes

@@ -255,31 +255,55 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
         float2 acc[8][2];
 #pragma unroll
         for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int s = 0; s < NC + B - 1; ++s) {
+        // window row s updates the candidates k = s - i it overlaps (block
+        // row i, accumulator k & 7); once its last row is in (s = k + 7)
+        // candidate k is emitted. SM8 = s & 7 and the range of i are
+        // compile-time, so the accumulators stay register names.
+        auto row = [&](int s, auto sm8_, auto ilo_, auto ihi_, auto emit_) {
+            constexpr int SM8 = decltype(sm8_)::value, ILO = decltype(ilo_)::value, IHI = decltype(ihi_)::value;
             const float2 p01 = make_float2(tile[s * kPitch + col[0]], tile[s * kPitch + col[1]]);
             const float2 p23 = make_float2(tile[s * kPitch + col[2]], tile[s * kPitch + col[3]]);
 #pragma unroll
-            for (int i = 0; i < B; ++i) {
-                const int k = s - i;
-                if (k >= 0 && k < NC) {
-                    // r - p exactly as fma(p, -1, r), then the square added
-                    const float2 d01 = __ffma2_rn(p01, neg1, ref[i][0]);
-                    const float2 d23 = __ffma2_rn(p23, neg1, ref[i][1]);
-                    acc[k & 7][0] = __ffma2_rn(d01, d01, acc[k & 7][0]);
-                    acc[k & 7][1] = __ffma2_rn(d23, d23, acc[k & 7][1]);
-                }
+            for (int i = ILO; i <= IHI; ++i) {
+                const int ks = (SM8 - i) & 7;
+                // r - p exactly as fma(p, -1, r), then the square added
+                const float2 d01 = __ffma2_rn(p01, neg1, ref[i][0]);
+                const float2 d23 = __ffma2_rn(p23, neg1, ref[i][1]);
+                acc[ks][0] = __ffma2_rn(d01, d01, acc[ks][0]);
+                acc[ks][1] = __ffma2_rn(d23, d23, acc[ks][1]);
             }
-            const int kd = s - (B - 1);
-            if (kd >= 0 && kd < NC) {
-                const float2 a = acc[kd & 7][0], b = acc[kd & 7][1];
-                acc[kd & 7][0] = acc[kd & 7][1] = make_float2(0.f, 0.f);
+            if constexpr (decltype(emit_)::value) {
+                constexpr int ks = (SM8 + 1) & 7;  // (s - 7) & 7
+                const int kd = s - (B - 1);
+                const float2 a = acc[ks][0], b = acc[ks][1];
+                acc[ks][0] = acc[ks][1] = make_float2(0.f, 0.f);
                 const float half_sum = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
                 const float dd = __fadd_rn(half_sum, __shfl_xor_sync(0xffffffffu, half_sum, 16));
                 stash[kd * (64 * P)] = dd;
                 pass |= Mask(dd > worst ? 0 : 1) << kd;
             }
+        };
+        // rows 0-6 (no candidate finished yet), then the rest: fully unrolled
+        // for small windows; for ranges from 25 on, the middle rows in a
+        // rolled loop of 8-row blocks so a column's code stays in the
+        // instruction cache, then the last rows
+        constexpr int NBLK = R >= 25 ? (NC - (B - 1)) / 8 : 0;
+        static_for<0, B - 1>([&](auto S_) {
+            constexpr int s = decltype(S_)::value;
+            row(s, ic<s & 7>(), ic<0>(), ic<(s < NC - 1 ? s : NC - 1)>(), ic<0>());
+        });
+#pragma unroll 1
+        for (int ob = 0; ob < NBLK; ++ob) {
+            static_for<0, 8>([&](auto U_) {
+                constexpr int u = decltype(U_)::value;
+                row(B - 1 + 8 * ob + u, ic<(B - 1 + u) & 7>(), ic<0>(), ic<B - 1>(), ic<1>());
+            });
         }
+        static_for<B - 1 + 8 * NBLK, NC + B - 1>([&](auto S_) {
+            constexpr int s = decltype(S_)::value;
+            row(s, ic<s & 7>(), ic<(s - NC + 1 > 0 ? s - NC + 1 : 0)>(), ic<(s < B - 1 ? s : B - 1)>(),
+                ic<(s >= B - 1)>());
+        });
         pass &= xok ? rows_ok : Mask(0);
         if (dxi == -ox && -oy >= 0 && -oy < NC) pass &= ~(Mask(1) << -oy);  // the reference itself
         while (pass) {

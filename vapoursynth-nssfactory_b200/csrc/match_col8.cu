@@ -217,46 +217,69 @@ __global__ void __launch_bounds__(32 * P, matchcol_min_blocks<K, P>()) matchcol_
             for (int h = 0; h < S2; ++h) a2[q][h] = make_float2(0.f, 0.f);
             a1[q] = 0.f;
         }
-#pragma unroll
-        for (int s = 0; s < NC + B - 1; ++s) {
+        // window row s updates the candidates k = s - i it overlaps (block
+        // row i, accumulator k & 7); once its last row is in (s = k + 7)
+        // candidate k is emitted. SM8 = s & 7 and the range of i are
+        // compile-time, so the accumulators stay register names.
+        auto row = [&](int s, auto sm8_, auto ilo_, auto ihi_, auto emit_) {
+            constexpr int SM8 = decltype(sm8_)::value, ILO = decltype(ilo_)::value, IHI = decltype(ihi_)::value;
             float2 p2[S2 > 0 ? S2 : 1];
 #pragma unroll
             for (int h = 0; h < S2; ++h)
                 p2[h] = make_float2(tile[s * kPitch + col[2 * h]], tile[s * kPitch + col[2 * h + 1]]);
             const float p1 = (S & 1) ? tile[s * kPitch + col[S - 1]] : 0.f;
 #pragma unroll
-            for (int i = 0; i < B; ++i) {
-                const int k = s - i;
-                if (k >= 0 && k < NC) {
+            for (int i = ILO; i <= IHI; ++i) {
+                const int ks = (SM8 - i) & 7;
 #pragma unroll
-                    for (int h = 0; h < S2; ++h) {
-                        const float2 d = __ffma2_rn(p2[h], neg1, rp[i][h]);
-                        a2[k & 7][h] = __ffma2_rn(d, d, a2[k & 7][h]);
-                    }
-                    if (S & 1) {
-                        const float d = __fmaf_rn(p1, -1.f, rs[i]);
-                        a1[k & 7] = __fmaf_rn(d, d, a1[k & 7]);
-                    }
+                for (int h = 0; h < S2; ++h) {
+                    const float2 d = __ffma2_rn(p2[h], neg1, rp[i][h]);
+                    a2[ks][h] = __ffma2_rn(d, d, a2[ks][h]);
+                }
+                if (S & 1) {
+                    const float d = __fmaf_rn(p1, -1.f, rs[i]);
+                    a1[ks] = __fmaf_rn(d, d, a1[ks]);
                 }
             }
-            const int kd = s - (B - 1);
-            if (kd >= 0 && kd < NC) {
+            if constexpr (decltype(emit_)::value) {
+                constexpr int ks = (SM8 + 1) & 7;  // (s - 7) & 7
+                const int kd = s - (B - 1);
                 float c[S];
 #pragma unroll
                 for (int h = 0; h < S2; ++h) {
-                    c[2 * h] = a2[kd & 7][h].x;
-                    c[2 * h + 1] = a2[kd & 7][h].y;
-                    a2[kd & 7][h] = make_float2(0.f, 0.f);
+                    c[2 * h] = a2[ks][h].x;
+                    c[2 * h + 1] = a2[ks][h].y;
+                    a2[ks][h] = make_float2(0.f, 0.f);
                 }
                 if (S & 1) {
-                    c[S - 1] = a1[kd & 7];
-                    a1[kd & 7] = 0.f;
+                    c[S - 1] = a1[ks];
+                    a1[ks] = 0.f;
                 }
                 const float dd = assemble<S>(c);
                 stash[kd * (32 * P)] = dd;
                 pass |= Mask(dd > worst ? 0 : 1) << kd;
             }
+        };
+        // rows 0-6: the first candidates, none finished yet
+        static_for<0, B - 1>([&](auto S_) {
+            constexpr int s = decltype(S_)::value;
+            row(s, ic<s & 7>(), ic<0>(), ic<s>(), ic<false>());
+        });
+        // rows 7 .. NC-1 in blocks of 8: every row updates 8 candidates and finishes one
+        constexpr int NBLK = (NC - (B - 1)) / 8;
+#pragma unroll 1
+        for (int ob = 0; ob < NBLK; ++ob) {
+            static_for<0, 8>([&](auto U_) {
+                constexpr int u = decltype(U_)::value;
+                row(B - 1 + 8 * ob + u, ic<(B - 1 + u) & 7>(), ic<0>(), ic<B - 1>(), ic<true>());
+            });
         }
+        // the remaining rows up to NC + 6: the last candidates finish
+        static_for<B - 1 + 8 * NBLK, NC + B - 1>([&](auto S_) {
+            constexpr int s = decltype(S_)::value;
+            row(s, ic<s & 7>(), ic<(s - NC + 1 > 0 ? s - NC + 1 : 0)>(), ic<(s < B - 1 ? s : B - 1)>(),
+                ic<(s >= B - 1)>());
+        });
         pass &= xok ? rows_ok : Mask(0);
         if (dxi == R) pass &= ~(Mask(1) << R);
         while (pass) {
