@@ -210,7 +210,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
     // Haar tubes, shrinkage, inverse Haar: positions lane and lane + 32
     int kept = 0;
     float w2 = 0.f;
-#pragma unroll
+#pragma unroll (G >= 16 ? 1 : 2)  // large groups: one copy of the tube code (instruction cache)
     for (int h = 0; h < 2; ++h) {
         const int f = lane + 32 * h, fa = Sh::at(f >> 3, f & 7);
         float t[G];
@@ -320,7 +320,7 @@ __device__ __forceinline__ void filter_group(float* cube, float* rcube, int lane
         }
         if (g < k && q == 0 && !win) add_weight(s, px, py, __float2ll_rn(wscaled));
         __syncwarp();
-#pragma unroll
+#pragma unroll (G >= 16 ? 1 : G)
         for (int gg = 0; gg < G; ++gg) {
             if (gg >= k) break;
             const int32_t pp = __shfl_sync(0xffffffffu, p, gg * Sh::LP);
