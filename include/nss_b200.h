@@ -107,7 +107,12 @@ typedef struct nssb_frame_out {
  * src/cuda/common/group_driver.cpp:1803 and :968-1107). clip_frames[i] (and
  * ref_frames[i], or NULL) are frames first+i, i < count, covering the
  * window above. memory says where all planes live. With NSSB_MEM_HOST the
- * copies to and from the device are part of the call. */
+ * copies to and from the device are part of the call. Several threads may
+ * call it at once on one handle (VapourSynth's fmParallel): a radius-0 frame
+ * takes one of the node's num_streams slots -- a stream and a set of frame
+ * buffers, the reference's slot pool (src/cuda/runtime/stream_pool.hpp:62-140)
+ * -- so the copies and kernels of frames on different slots overlap, and
+ * waits while all slots are busy; temporal frames run one at a time. */
 int nssb_bm3d_get_frame(nssb_bm3d* h, int n, const nssb_frame* clip_frames, const nssb_frame* ref_frames, int first,
                         int count, int memory, nssb_frame_out* out);
 
