@@ -347,7 +347,9 @@ def our_arm(args):
                                "note": "plain form, one pass over the step's frames"},
         "clocks": clock,
     }
-    if not args.no_legs:
+    # the other configs' legs run at one GPU (the scaling runs time the headline only)
+    legs = not args.no_legs and world == 1
+    if legs:
         out["reference_gpu"] = reference_gpu_leg(nssb, dframes, dout, args.steps, args.warmup)
         out["reference_gpu"]["ours_batched_over_reference"] = value / out["reference_gpu"]["fps"] \
             if "fps" in out["reference_gpu"] else None
@@ -362,7 +364,7 @@ def our_arm(args):
     node_h.close()
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    if args.served > 0 and not args.no_legs:
+    if args.served > 0 and legs:
         out["served"] = served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
                                    args.served_workers)
         out["served"]["workers"] = args.served_workers
