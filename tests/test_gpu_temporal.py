@@ -146,3 +146,45 @@ def test_frame_props(nssb, synth, dev):
     assert nssb.BM3D(clip, sigma=10, radius=1).frame_props(2) == base  # rolling: finished frames
     fat = nssb.BM3D(clip, sigma=10, radius=1, temporal_mode="legacy").frame_props(2)
     assert fat == {**base, "_NSSFatVersion": 2, "_NSSFatRadius": 1, "_NSSFatCenter": 2, "_NSSFatLayout": 1}
+
+
+def test_temporal_planes_8192_and_wider(nssb, oracle, synth, dev):
+    """Planes 8192 and more pixels wide take the generic temporal kernel
+    (16-bit coordinates); its match lists equal the oracle's, refs past
+    x = 8192 included, and the rolling output of a node keeps the 60 dB bar."""
+    radius, block, group, rng_, ps_num, ps_range, step = 1, 8, 8, 9, 2, 4, 8
+    ntemp = 2 * radius + 1
+    frames = gray_clip(synth, ntemp, 8232, 24, 10, seed=17)
+    h, w = frames[0].shape
+    dframes = [torch.from_numpy(f).to(dev) for f in frames]
+    nx, ny = (w - block + step - 1) // step + 1, (h - block + step - 1) // step + 1
+    pos = torch.full((nx * ny, group), -7, dtype=torch.int32, device=dev)
+    slot = torch.full((nx * ny, group), -7, dtype=torch.int32, device=dev)
+    dist = torch.zeros((nx * ny, group), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(nx * ny, dtype=torch.int32, device=dev)
+    ptrs = (C.c_void_p * ntemp)(*[f.data_ptr() for f in dframes])
+    strides = (C.c_int64 * ntemp)(*([w] * ntemp))
+    nssb.check(nssb.lib().nssb_match_temporal(ptrs, strides, ntemp, radius, 0, -1, w, h, block, step, rng_, group,
+                                              ps_num, ps_range, pos.data_ptr(), slot.data_ptr(), dist.data_ptr(),
+                                              cnt.data_ptr(), None))
+    torch.cuda.synchronize()
+    pos, slot, dist, cnt = pos.cpu().numpy(), slot.cpu().numpy(), dist.cpu().numpy(), cnt.cpu().numpy()
+    rs = np.random.default_rng(3)
+    jobs = [j for j in range(nx * ny) if min((j % nx) * step, w - block) >= 8150]
+    jobs += list(rs.choice(nx * ny, 120, replace=False))
+    assert any(int(p) & 0xFFFF >= 8192 for j in jobs for p in pos[j][:cnt[j]])
+    for j in jobs:
+        bx, by = min((j % nx) * step, w - block), min((j // nx) * step, h - block)
+        want = oracle.predictive_match(frames, bx, by, radius, block=block, group=group, bm_range=rng_,
+                                       radius=radius, ps_num=ps_num, ps_range=ps_range, step=step)
+        assert cnt[j] == len(want), (j, cnt[j], len(want))
+        got = [(int(p) & 0xFFFF, int(p) >> 16, int(t), float(d)) for p, t, d in zip(pos[j], slot[j], dist[j])]
+        assert got[:cnt[j]] == [(m[0], m[1], m[2], m[3]) for m in want], j
+
+    clip = nssb.Clip.from_frames([(f,) for f in frames], nssb.GRAY)
+    node = nssb.BM3D(clip, sigma=10, radius=radius)
+    got = node.get_frame(1)[0]
+    node.close()
+    st = oracle.stage(oracle.effective_sigma(10.0))
+    want = oracle.bm3d_clip_plane(frames, st, radius)[1]
+    assert oracle.psnr(got, want) >= MIN_PSNR

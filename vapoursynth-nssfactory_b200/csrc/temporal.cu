@@ -18,8 +18,15 @@ namespace {
 
 struct TKey {
     uint32_t d;    // canonical distance bits
-    uint32_t tyx;  // slot << 26 | y << 13 | x  (x, y < 8192)
+    uint64_t tyx;  // slot << 32 | y << 16 | x  (x, y < 65536)
 };
+
+__device__ __forceinline__ uint64_t tyx_key(int t, int y, int x) {
+    return (uint64_t(uint32_t(t)) << 32) | (uint64_t(uint32_t(y)) << 16) | uint64_t(uint32_t(x));
+}
+__device__ __forceinline__ int tyx_x(uint64_t k) { return int(k & 0xffffu); }
+__device__ __forceinline__ int tyx_y(uint64_t k) { return int((k >> 16) & 0xffffu); }
+__device__ __forceinline__ int tyx_t(uint64_t k) { return int(k >> 32); }
 
 __device__ __forceinline__ bool tkey_less(const TKey& a, const TKey& b) {
     return a.d != b.d ? a.d < b.d : a.tyx < b.tyx;
@@ -106,14 +113,14 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
     const int nseed = min(n, ps_num);
     for (int i = 0; i < nseed; ++i) {
         seeds[i].d = canon(od[i]);
-        seeds[i].tyx = (uint32_t(t0) << 26) | (uint32_t(pos_y(op[i])) << 13) | uint32_t(pos_x(op[i]));
+        seeds[i].tyx = tyx_key(t0, pos_y(op[i]), pos_x(op[i]));
     }
     TList global;
     global.init(G - 1);
     for (int i = 1; i < n; ++i) {
         TKey k;
         k.d = canon(od[i]);
-        k.tyx = (uint32_t(t0) << 26) | (uint32_t(pos_y(op[i])) << 13) | uint32_t(pos_x(op[i]));
+        k.tyx = tyx_key(t0, pos_y(op[i]), pos_x(op[i]));
         global.add(k);
     }
     const int maxx = W - blk, maxy = H - blk;
@@ -129,7 +136,7 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
             local.init(min(ps_num, G));
             int ymin = H, ymax = -1;
             for (int i = 0; i < nc; ++i) {
-                const int cyy = (centers[i].tyx >> 13) & 0x1fff;
+                const int cyy = tyx_y(centers[i].tyx);
                 ymin = min(ymin, max(0, cyy - ps_range));
                 ymax = max(ymax, min(maxy, cyy + ps_range));
             }
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
                 // the x intervals of the windows that cover row y, in ascending order
                 int ia[64], ib[64], ni = 0;
                 for (int i = 0; i < nc; ++i) {
-                    const int cyy = (centers[i].tyx >> 13) & 0x1fff, cxx = centers[i].tyx & 0x1fff;
+                    const int cyy = tyx_y(centers[i].tyx), cxx = tyx_x(centers[i].tyx);
                     if (abs(y - cyy) <= ps_range) {
                         const int a = max(0, cxx - ps_range), b = min(maxx, cxx + ps_range);
                         int p = ni++;
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
                         }
                         TKey k;
                         k.d = canon(d);
-                        k.tyx = (uint32_t(t) << 26) | (uint32_t(y) << 13) | uint32_t(x);
+                        k.tyx = tyx_key(t, y, x);
                         local.add(k);
                     }
                     done = max(done, ib[i]);
@@ -182,8 +189,8 @@ __global__ void __launch_bounds__(64) temporal_kernel(TemporalPlanes tp, int nte
     for (int q = 0; q < G - 1; ++q) {
         const bool valid = q < global.n;
         const TKey k = global.k[q];
-        op[1 + q] = valid ? pack_pos(k.tyx & 0x1fff, (k.tyx >> 13) & 0x1fff) : -1;
-        os[1 + q] = valid ? int32_t(k.tyx >> 26) : -1;
+        op[1 + q] = valid ? pack_pos(tyx_x(k.tyx), tyx_y(k.tyx)) : -1;
+        os[1 + q] = valid ? tyx_t(k.tyx) : -1;
         od[1 + q] = valid ? __uint_as_float(k.d) : 0.f;
     }
     os[0] = t0;
@@ -652,15 +659,15 @@ bool launch_match_temporal_batch(TemporalBatch& tb, cudaStream_t stream) {
 void launch_match_temporal(const TemporalPlanes& planes, int ntemp, int t0, int valid_begin, int valid_end,
                            int width, int height, int block, int step, int group, int ps_num, int ps_range,
                            int32_t* pos, int32_t* slot, float* dist, int32_t* count, cudaStream_t stream) {
-    if (width >= 8192 || height >= 8192) throw std::invalid_argument("nss_cuda: temporal planes must be < 8192 wide");
     const int nx = grid_count(width, block, step), ny = grid_count(height, block, step);
     const int jobs = nx * ny;
     if (jobs == 0) return;
     const int first = valid_begin < 0 ? 0 : valid_begin;
     const int last = valid_end < 0 ? ntemp : (valid_end < ntemp ? valid_end : ntemp);
     const int layers = (ntemp - 1) / 2;
+    // the fast path packs slot, y and x into 6 + 13 + 13 bits; larger planes take the generic kernel
     if (block == 8 && ps_num <= 8 && ps_range <= 12 && group <= 64 && 2 * layers * ps_num <= 2 * 16 * 8 &&
-        ntemp <= 33) {
+        ntemp <= 33 && width < 8192 && height < 8192) {
         const dim3 g8(ceil_div(jobs, kTRefs));
         auto go = [&](auto kern) {
             kern<<<g8, 32 * kTRefs, 0, stream>>>(planes, ntemp, t0, first, last, width, height, group, ps_num,
