@@ -60,7 +60,8 @@ def parse():
                     help="skip the temporal (C3), mixed-batch (C4) and served legs (profiling runs)")
     ap.add_argument("--served-workers", type=int, default=8, help="temporal requests the server runs at once")
     ap.add_argument("--c3-frames", type=int, default=60)
-    ap.add_argument("--only", choices=["c3", "c4", "served", "refgpu", "heavy"], help="run one leg alone (profiling)")
+    ap.add_argument("--only", choices=["c3", "c4", "served", "refgpu", "heavy", "wide"],
+                    help="run one leg alone (profiling)")
     ap.add_argument("--served-plain", type=int, default=300,
                     help="requests of the same stream rendered by the per-frame drop-in for comparison")
     return ap.parse_args()
@@ -228,7 +229,8 @@ def our_arm(args):
                 "served": lambda: served_leg(nssb, synth, local, args.served, min(args.served, args.served_plain),
                                              args.served_workers),
                 "refgpu": lambda: refgpu_only(nssb, synth, dev, args),
-                "heavy": lambda: heavy_only(nssb, synth, dev, args)}
+                "heavy": lambda: heavy_only(nssb, synth, dev, args),
+                "wide": lambda: wide_window_leg(nssb, synth, dev)}
         print(json.dumps({"leg": args.only, **legs[args.only]()}), flush=True)
         return
     nf = args.frames
@@ -356,6 +358,7 @@ def our_arm(args):
         out["reference_gpu"]["ours_plain_over_reference"] = plain_value / out["reference_gpu"]["fps"] \
             if "fps" in out["reference_gpu"] else None
         out["temporal_c3"] = c3_leg(nssb, synth, dev, args.c3_frames, rank == 0 and world == 1 and not args.no_cpu)
+        out["precision_wide"] = wide_window_leg(nssb, synth, dev)
         out["batched_c4"] = c4_leg(nssb, synth, dev, check_psnr=rank == 0 and world == 1 and not args.no_cpu)
     # the headline's batch layouts and nodes are released before the served
     # leg sizes its memory budget from the device's free memory
@@ -492,6 +495,56 @@ def heavy_only(nssb, synth, dev, args):
     torch.cuda.synchronize()
     node.close()
     return {"heavy_fps": len(dframes) * args.steps / (s.elapsed_time(e) / 1e3), "frames": len(dframes)}
+
+
+def wide_window_leg(nssb, synth, dev, n_frames=4):
+    """The precision form at large search windows against the FP32 matchers:
+    the reference's "heavy" preset (final=1, block_step=3, group_size=32,
+    group_size_basic=16, bm_range=19) and final=1 at bm_range 25 and 31 on
+    1080p YUV420 frames of the headline generator; per-frame drop-in, matcher
+    time per frame (CUDA events around each matching launch), whole frames/s,
+    outputs compared bit for bit between the forms."""
+    import torch
+
+    frames = synth.yuv420_clip(1000, W, H, n_frames, SIGMA)
+    dframes = [tuple(torch.from_numpy(p).to(dev) for p in f) for f in frames]
+    shapes = {"heavy": dict(final=1, block_step=3, group_size=32, group_size_basic=16, bm_range=19),
+              "bm_range_25": dict(final=1, bm_range=25), "bm_range_31": dict(final=1, bm_range=31)}
+    res = {}
+    for name, kw in shapes.items():
+        outs, row = {}, {}
+        for form in (0, 1):
+            node = nssb.BM3D(nssb.Clip.from_frames(dframes, nssb.YUV, 1, 1), sigma=SIGMA, **kw)
+            node.set_matcher(form)
+            out = [tuple(torch.empty_like(p) for p in f) for f in dframes]
+            for n in range(len(dframes)):
+                node.get_frame(n, out=out[n])
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            for n in range(len(dframes)):
+                node.get_frame(n, out=out[n])
+            e.record()
+            torch.cuda.synchronize()
+            fps = len(dframes) / (s.elapsed_time(e) / 1e3)
+            node.stats(True, True)
+            for n in range(len(dframes)):
+                node.get_frame(n, out=out[n])
+            torch.cuda.synchronize()
+            st = node.stats(False, False)
+            node.close()
+            outs[form] = out
+            tag = "tensor" if form else "fp32"
+            row[f"{tag}_fps"] = fps
+            row[f"{tag}_match_ms_per_frame"] = st.match_ms / len(dframes)
+            if form:
+                row["survivors_per_reference"] = st.tc_survivors / max(1, st.tc_refs)
+                row["max_error_over_margin"] = st.tc_max_error_ratio
+        row["bit_identical"] = all(torch.equal(a, b) for fa, fb in zip(outs[0], outs[1]) for a, b in zip(fa, fb))
+        row["args"] = kw
+        res[name] = row
+    res["frames"] = len(dframes)
+    return res
 
 
 def refgpu_only(nssb, synth, dev, args):

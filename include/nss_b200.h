@@ -178,8 +178,9 @@ int nssb_bm3d_set_window(nssb_bm3d* h, float beta);
 int nssb_match_spatial(const float* plane, int64_t stride, int width, int height, int block, int step,
                        int bm_range, int group, int32_t* pos, float* dist, int32_t* count, void* stream);
 
-/* Precision form of nssb_match_spatial for 8x8 blocks and bm_range 9 (groups
- * 2, 4, 8, 16): candidate distances |r|^2 + |c|^2 - 2 r.c with the dot
+/* Precision form of nssb_match_spatial for 8x8 blocks, bm_range 9 (groups 2,
+ * 4, 8, 16) and bm_range 10-64 (groups 2-32): candidate distances
+ * |r|^2 + |c|^2 - 2 r.c with the dot
  * products on the tensor cores (tcgen05.mma, BF16 hi/lo split of every pixel,
  * FP32 accumulation in tensor memory), then every candidate within a proven
  * error margin of the K-th distance re-ranked with the exact FP32 distance,
@@ -196,8 +197,9 @@ typedef struct nssb_tc_stats {
     int flagged_tiles;      /* tiles with non-finite pixels (every candidate re-ranked) */
     int timeouts;           /* bounded device waits that gave up */
 } nssb_tc_stats;
-int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int group,
-                          int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats, void* stream);
+int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int bm_range,
+                          int group, int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats,
+                          void* stream);
 
 /* Predictive temporal matching (collect_temporal, matcher.hpp:319-373; device
  * form match.cu:1707-1757). planes/strides: host arrays of ntemp device

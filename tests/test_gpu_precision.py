@@ -29,7 +29,7 @@ def grid(n, b, s):
     return (n - b + s - 1) // s + 1
 
 
-def run_both(nssb, img, dev, step=8, group=8):
+def run_both(nssb, img, dev, step=8, group=8, bm_range=9):
     h, w = img.shape
     plane = torch.from_numpy(np.ascontiguousarray(img, np.float32)).to(dev)
     jobs = grid(w, 8, step) * grid(h, 8, step)
@@ -40,10 +40,10 @@ def run_both(nssb, img, dev, step=8, group=8):
         dist = torch.full((jobs, group), -7.0, dtype=torch.float32, device=dev)
         cnt = torch.zeros(jobs, dtype=torch.int32, device=dev)
         if tc:
-            rc = nssb.lib().nssb_match_spatial_tc(plane.data_ptr(), w, w, h, step, group, pos.data_ptr(),
+            rc = nssb.lib().nssb_match_spatial_tc(plane.data_ptr(), w, w, h, step, bm_range, group, pos.data_ptr(),
                                                   dist.data_ptr(), cnt.data_ptr(), C.byref(stats), None)
         else:
-            rc = nssb.lib().nssb_match_spatial(plane.data_ptr(), w, w, h, 8, step, 9, group, pos.data_ptr(),
+            rc = nssb.lib().nssb_match_spatial(plane.data_ptr(), w, w, h, 8, step, bm_range, group, pos.data_ptr(),
                                                dist.data_ptr(), cnt.data_ptr(), None)
         nssb.check(rc)
         torch.cuda.synchronize()
@@ -129,3 +129,46 @@ def test_engine_precision_form_same_frames(nssb, synth, dev):
         assert st.tc_refs > 0 and st.tc_max_error_ratio < 1.0
         a.close()
         b.close()
+
+
+# bm_range 10-64: the references on the MMA's M side (match_tcw.cu)
+@pytest.mark.parametrize("w,h,step,rng_,group,sigma", [
+    (160, 96, 3, 19, 16, 10), (160, 96, 3, 19, 32, 10), (200, 120, 8, 25, 8, 5), (131, 77, 4, 16, 4, 20),
+    (300, 90, 8, 31, 8, 10), (96, 200, 2, 12, 2, 10), (257, 130, 5, 40, 32, 5), (150, 90, 1, 10, 16, 10),
+    (400, 150, 8, 64, 8, 10), (88, 72, 6, 20, 32, 3),
+])
+def test_large_window_equals_fp32_matcher(nssb, synth, dev, w, h, step, rng_, group, sigma):
+    img = synth.gray_frame(w * 5 + h + rng_, w, h, sigma)[0]
+    out, st = run_both(nssb, img, dev, step, group, rng_)
+    print(f"{w}x{h} step {step} range {rng_} group {group}: {st.survivors / max(1, st.refs):.1f} survivors "
+          f"per reference, max error/margin {st.max_error_ratio:.4f}")
+    assert st.timeouts == 0 and st.flagged_tiles == 0
+    assert_equal_lists(out)
+    assert st.refs == grid(w, 8, step) * grid(h, 8, step)
+    assert st.max_error_ratio < 1.0
+
+
+@pytest.mark.parametrize("rng_,group", [(19, 16), (25, 32)])
+def test_large_window_ties_and_non_finite(nssb, synth, dev, rng_, group):
+    flat = np.full((72, 136), 0.25, np.float32)
+    out, _ = run_both(nssb, flat, dev, 3, group, rng_)
+    assert_equal_lists(out)
+    rng = np.random.default_rng(rng_)
+    quant = (rng.integers(0, 4, (90, 150)) / 4.0).astype(np.float32)
+    out, _ = run_both(nssb, quant, dev, 4, group, rng_)
+    assert_equal_lists(out)
+    img = synth.gray_frame(13, 140, 100, 10)[0]
+    img[10, 20] = np.nan
+    img[60, 120] = np.inf
+    out, st = run_both(nssb, img, dev, 3, group, rng_)
+    assert st.flagged_tiles > 0
+    assert_equal_lists(out)
+
+
+def test_heavy_preset_1080p_plane(nssb, synth, dev):
+    # the "heavy" preset's matching shapes (block_step 3, bm_range 19, groups 16 and 32) on a 1080p luma plane
+    img = synth.yuv420_clip(9, 1920, 1080, 1, 5.0)[0][0]
+    for group in (16, 32):
+        out, st = run_both(nssb, img, dev, 3, group, 19)
+        assert_equal_lists(out)
+        assert st.max_error_ratio < 1.0 and st.timeouts == 0

@@ -174,8 +174,8 @@ def lib():
         L.nssb_bm3d_set_matcher.argtypes = [C.c_void_p, C.c_int]
         L.nssb_bm3d_set_window.argtypes = [C.c_void_p, C.c_float]
         L.nssb_bm3d_frame_props.argtypes = [C.c_void_p, C.c_int, C.POINTER(Prop), C.c_int, C.POINTER(C.c_int)]
-        L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
-                                            C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
+        L.nssb_match_spatial_tc.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(TcStats), C.c_void_p]
         L.nssb_batch_create.argtypes = [C.c_int, C.POINTER(Arg), C.c_int, C.POINTER(C.c_void_p)]
         L.nssb_batch_run.argtypes = [C.c_void_p, C.POINTER(BatchItem), C.c_int]
         L.nssb_batch_get_info.argtypes = [C.c_void_p, C.POINTER(BatchInfo)]

@@ -222,8 +222,9 @@ int nssb_bm3d_set_matcher(nssb_bm3d* h, int form) {
     });
 }
 
-int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int group,
-                          int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats, void* stream) {
+int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int height, int step, int bm_range,
+                          int group, int32_t* pos, float* dist, int32_t* count, nssb_tc_stats* stats,
+                          void* stream) {
     int timeouts = 0;
     const int rc = guarded([&] {
         if (!plane || !pos || !count || width < 8 || height < 8 || step < 1 || step > 8 || stride < width)
@@ -236,12 +237,15 @@ int nssb_match_spatial_tc(const float* plane, int64_t stride, int width, int hei
         mb->n = 1;
         mb->step = step;
         mb->p[0] = nssb::MatchPlane{plane, stride, pos, dist, count, width, height, 0, 0, 0};
-        const bool ok = nssb::launch_match_tc_batch(*mb, 9, group, ctr, s);
+        const bool ok = nssb::launch_match_tc_batch(*mb, bm_range, group, ctr, s);
         nssb::TcCounters host{};
         if (ok) NSSB_CUDA(cudaMemcpyAsync(&host, ctr, sizeof host, cudaMemcpyDeviceToHost, s));
         NSSB_CUDA(cudaFreeAsync(ctr, s));
         NSSB_CUDA(cudaStreamSynchronize(s));
-        if (!ok) throw std::invalid_argument("nss_cuda: the precision matcher covers 8x8 blocks, bm_range 9, groups 2/4/8/16");
+        if (!ok)
+            throw std::invalid_argument(
+                "nss_cuda: the precision matcher covers 8x8 blocks, bm_range 9 (groups 2/4/8/16) and bm_range "
+                "10-64 (groups 2/4/8/16/32)");
         timeouts = (int)host.timeouts;
         if (stats) {
             stats->survivors = (int64_t)host.survivors;

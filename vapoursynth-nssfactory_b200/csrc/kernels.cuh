@@ -71,7 +71,10 @@ struct TcCounters {
     unsigned long long survivors, refs;
     unsigned int max_ratio_bits, flagged_tiles, timeouts, pad;
 };
+// The precision form: bm_range 9 on match_tc.cu's kernel, 10-64 on match_tcw.cu's
+// (references on the MMA's M side); false where neither covers the shape.
 bool launch_match_tc_batch(MatchBatch& batch, int bm_range, int group, TcCounters* counters, cudaStream_t stream);
+bool launch_match_tcw_batch(MatchBatch& batch, int bm_range, int group, TcCounters* counters, cudaStream_t stream);
 
 struct GroupPlane {
     const float* src;

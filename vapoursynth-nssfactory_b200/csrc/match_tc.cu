@@ -32,13 +32,14 @@
 // (src/cuda/common/match.cu, mma.sync path; docs/api/cuda/bm3d.md:20-59) --
 // this one is tcgen05/TMEM-based and exact.
 #include "kernels.cuh"
-
-#include <cuda_bf16.h>
+#include "tcgen05.cuh"
 
 #include <algorithm>
 
 namespace nssb {
 namespace {
+
+using namespace tc;
 
 constexpr int kTcRefs = 14;
 constexpr int kTcThreads = 256;
@@ -63,70 +64,8 @@ struct Tc {
     static constexpr int BYTES = TILE + RB * TP * 4;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// UMMA shared-memory descriptor, no swizzle (layout type 0), sm_100 version 1.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A (MN-major) and B
-// (K-major), M = 128, N = 16.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, bool acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        :
-        : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"((uint32_t)acc));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-// Bounded wait on an mbarrier phase; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint32_t a = smem_u32(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t addr, float v[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
-}
-
-
-// bf16 hi/lo of two floats, packed (low half = first).
-__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
-    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    const float2 hf = __bfloat1622float2(h);
-    const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
-    hi = *reinterpret_cast<const uint32_t*>(&h);
-    lo = *reinterpret_cast<const uint32_t*>(&l);
-}
+// kind::f16: F32 accumulate, BF16 A (MN-major) and B (K-major), M = 128, N = 16.
+constexpr uint32_t kIdesc = tc::idesc_bf16(128, 16, true, false);
 
 __device__ __forceinline__ uint64_t tc_key(float d, int x, int y) {
     uint32_t b = __float_as_uint(d);
@@ -206,9 +145,9 @@ __device__ __forceinline__ void issue_row(uint32_t smem0, uint32_t tmem, int c, 
         const uint64_t al = umma_desc(smem0 + T::A_LO + arow, kBlockBytes, 128);
         const uint64_t bh = umma_desc(smem0 + T::B_HI + s * 256, 128, 1024);
         const uint64_t bl = umma_desc(smem0 + T::B_LO + s * 256, 128, 1024);
-        mma_bf16(tmem, ah, bh, s > 0);
-        mma_bf16(tmem, ah, bl, true);
-        mma_bf16(tmem, al, bh, true);
+        mma_bf16(tmem, ah, bh, kIdesc, s > 0);
+        mma_bf16(tmem, ah, bl, kIdesc, true);
+        mma_bf16(tmem, al, bh, kIdesc, true);
     }
     mma_commit(bar);
 }
@@ -521,7 +460,8 @@ void launch_tc(MatchBatch& mb, TcCounters* ctr, cudaStream_t stream) {
 }  // namespace
 
 bool launch_match_tc_batch(MatchBatch& mb, int bm_range, int group, TcCounters* counters, cudaStream_t stream) {
-    if (!counters || mb.step < 1 || mb.step > 8 || mb.n < 1 || mb.n > kMaxBatchPlanes || bm_range != 9) return false;
+    if (!counters || mb.step < 1 || mb.step > 8 || mb.n < 1 || mb.n > kMaxBatchPlanes) return false;
+    if (bm_range != 9) return launch_match_tcw_batch(mb, bm_range, group, counters, stream);
     for (int i = 0; i < mb.n; ++i)
         if (mb.p[i].W < 8 || mb.p[i].H < 8 || mb.p[i].W > 65535 || mb.p[i].H > 65535) return false;
     switch (group) {
