@@ -500,7 +500,8 @@ def heavy_only(nssb, synth, dev, args):
 def wide_window_leg(nssb, synth, dev, n_frames=4):
     """The precision form at large search windows against the FP32 matchers:
     the reference's "heavy" preset (final=1, block_step=3, group_size=32,
-    group_size_basic=16, bm_range=19) and final=1 at bm_range 25 and 31 on
+    group_size_basic=16, bm_range=19) and final=1 at bm_range 25, 31, 40 and
+    64 (step 8) and 40 (step 4) on
     1080p YUV420 frames of the headline generator; per-frame drop-in, matcher
     time per frame (CUDA events around each matching launch), whole frames/s,
     outputs compared bit for bit between the forms."""
@@ -509,7 +510,9 @@ def wide_window_leg(nssb, synth, dev, n_frames=4):
     frames = synth.yuv420_clip(1000, W, H, n_frames, SIGMA)
     dframes = [tuple(torch.from_numpy(p).to(dev) for p in f) for f in frames]
     shapes = {"heavy": dict(final=1, block_step=3, group_size=32, group_size_basic=16, bm_range=19),
-              "bm_range_25": dict(final=1, bm_range=25), "bm_range_31": dict(final=1, bm_range=31)}
+              "bm_range_25": dict(final=1, bm_range=25), "bm_range_31": dict(final=1, bm_range=31),
+              "bm_range_40": dict(final=1, bm_range=40), "bm_range_64": dict(final=1, bm_range=64),
+              "bm_range_40_step_4": dict(final=1, bm_range=40, block_step=4)}
     res = {}
     for name, kw in shapes.items():
         outs, row = {}, {}

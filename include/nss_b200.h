@@ -149,10 +149,14 @@ typedef struct nssb_kernel_stats {
 int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stats* out);
 
 /* Matcher of a handle's 8x8 stages (spatial and the centre frame of
- * temporal): 0 = FP32 (default), 1 = the tensor-core precision form of
- * nssb_match_spatial_tc. Outputs are bit-identical either way. */
+ * temporal): 0 = FP32, 1 = the tensor-core precision form of
+ * nssb_match_spatial_tc, 2 = automatic (the default): the precision form
+ * from bm_range 32 on, where it measured faster, FP32 below. Outputs are
+ * bit-identical whichever form runs. No reference counterpart (the
+ * reference picks its CUDA matcher by shape, src/cuda/common/match.cu:1605-1611). */
 #define NSSB_MATCHER_FP32 0
 #define NSSB_MATCHER_TENSOR 1
+#define NSSB_MATCHER_AUTO 2
 int nssb_bm3d_set_matcher(nssb_bm3d* h, int form);
 
 /* Opt-in Kaiser aggregation window. No counterpart in the reference's BM3D,

@@ -172,3 +172,20 @@ def test_heavy_preset_1080p_plane(nssb, synth, dev):
         out, st = run_both(nssb, img, dev, 3, group, 19)
         assert_equal_lists(out)
         assert st.max_error_ratio < 1.0 and st.timeouts == 0
+
+
+def test_automatic_matcher_form(nssb, synth, dev):
+    # the default form takes the precision form from bm_range 32 on and the FP32 matcher below;
+    # the output is the FP32 form's bit for bit either way
+    frames = synth.yuv420_clip(31, 256, 144, 1, 10.0)
+    clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
+    for rng_, tensor in ((40, True), (16, False)):
+        auto, fp32 = nssb.BM3D(clip, sigma=10, final=1, bm_range=rng_), nssb.BM3D(clip, sigma=10, final=1, bm_range=rng_)
+        fp32.set_matcher(0)
+        auto.stats(True, True)
+        a, b = auto.get_frame(0), fp32.get_frame(0)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+        st = auto.stats(False, False)
+        assert (st.tc_refs > 0) == tensor
+        auto.close()
+        fp32.close()

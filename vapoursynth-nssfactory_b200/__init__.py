@@ -324,7 +324,8 @@ class Node:
         return {arr[i].key.decode(): arr[i].value for i in range(k.value)}
 
     def set_matcher(self, form: int) -> None:
-        """0: FP32 matcher (default); 1: tensor-core precision form (identical lists)."""
+        """0: FP32 matcher; 1: tensor-core precision form; 2: automatic (the default: the precision
+        form from bm_range 32 on, FP32 below). Identical lists whichever runs."""
         check(lib().nssb_bm3d_set_matcher(self.handle, int(form)))
 
     def set_window(self, beta: float) -> None:

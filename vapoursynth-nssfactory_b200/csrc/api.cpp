@@ -216,8 +216,9 @@ int nssb_bm3d_set_window(nssb_bm3d* h, float beta) {
 int nssb_bm3d_set_matcher(nssb_bm3d* h, int form) {
     return guarded([&] {
         if (!h) throw std::invalid_argument("nssb_bm3d_set_matcher: invalid handle");
-        if (form != NSSB_MATCHER_FP32 && form != NSSB_MATCHER_TENSOR)
-            throw std::invalid_argument("nssb_bm3d_set_matcher: form must be NSSB_MATCHER_FP32 or NSSB_MATCHER_TENSOR");
+        if (form != NSSB_MATCHER_FP32 && form != NSSB_MATCHER_TENSOR && form != NSSB_MATCHER_AUTO)
+            throw std::invalid_argument(
+                "nssb_bm3d_set_matcher: form must be NSSB_MATCHER_FP32, NSSB_MATCHER_TENSOR or NSSB_MATCHER_AUTO");
         h->engine->set_matcher(form);
     });
 }

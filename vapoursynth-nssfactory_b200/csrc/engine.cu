@@ -141,6 +141,13 @@ void Engine::give_back(Slot* s) {
 
 void Engine::alloc() {
     for (auto& s : slots_) alloc_slot(*s);
+    // the automatic matcher form (the default) may take the precision form: its counters
+    auto* c = static_cast<TcCounters*>(dev_alloc(sizeof(TcCounters)));
+    allocations_.push_back(c);
+    NSSB_CUDA(cudaMemsetAsync(c, 0, sizeof(TcCounters), stream_));
+    NSSB_CUDA(cudaStreamSynchronize(stream_));
+    tunes_.match.tc = c;
+    tunes_.match.form = 2;
 }
 
 void Engine::alloc_slot(Slot& s) {
@@ -264,7 +271,7 @@ void Engine::set_matcher(int form) {
     // every slot idle: no frame may be reading the tunes
     std::vector<Slot*> held;
     for (size_t i = 0; i < slots_.size(); ++i) held.push_back(lease(false));
-    if (form == 1 && !tunes_.match.tc) {
+    if (form != 0 && !tunes_.match.tc) {
         auto* c = static_cast<TcCounters*>(dev_alloc(sizeof(TcCounters)));
         allocations_.push_back(c);
         NSSB_CUDA(cudaMemsetAsync(c, 0, sizeof(TcCounters), stream_));

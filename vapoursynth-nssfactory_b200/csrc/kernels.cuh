@@ -46,7 +46,8 @@ struct MatchTune {
     int parts = 2;           // warp pairs splitting the window columns: 1, 2 or 4
     int persistent = 0;      // 1: one resident wave taking tiles from a device counter
     int* queue = nullptr;    // that counter (one int of device memory)
-    int form = 0;            // 0: FP32 SIMT matcher; 1: tensor-core distances + exact re-rank (same lists)
+    int form = 0;            // 0: FP32 SIMT matcher; 1: tensor-core distances + exact re-rank (same lists);
+                             // 2: automatic, the form that measured faster for the shape
     TcCounters* tc = nullptr;  // counters of the tensor form (device memory)
 };
 // The specialised exact matcher for 8x8 blocks (match8.cu) over a batch of
@@ -71,6 +72,12 @@ struct TcCounters {
     unsigned long long survivors, refs;
     unsigned int max_ratio_bits, flagged_tiles, timeouts, pad;
 };
+// Whether a stage of 8x8 blocks with this search range takes the precision
+// form: asked for (form 1), or automatically (form 2) from bm_range 32 on,
+// where the FP32 matcher sweeps the window in bands and the tensor form
+// measured 1.3-2.8x faster on 1080p YUV420 frames (steps 3-8, ranges 32-64;
+// below range 32 the FP32 matchers are faster). Lists are identical either way.
+inline bool tensor_matcher_takes(int form, int bm_range) { return form == 1 || (form == 2 && bm_range >= 32); }
 // The precision form: bm_range 9 on match_tc.cu's kernel, 10-64 on match_tcw.cu's
 // (references on the MMA's M side); false where neither covers the shape.
 bool launch_match_tc_batch(MatchBatch& batch, int bm_range, int group, TcCounters* counters, cudaStream_t stream);
