@@ -189,3 +189,14 @@ def test_automatic_matcher_form(nssb, synth, dev):
         assert (st.tc_refs > 0) == tensor
         auto.close()
         fp32.close()
+
+
+@pytest.mark.parametrize("w,h", [(8, 8), (9, 40), (40, 9), (300, 8), (13, 200), (71, 67)])
+@pytest.mark.parametrize("step,rng_,group", [(1, 32, 2), (8, 64, 32), (3, 40, 16)])
+def test_large_window_small_and_thin_planes(nssb, synth, dev, w, h, step, rng_, group):
+    rs = np.random.default_rng(w * 1000 + h + rng_)
+    img = (rs.random((h, w)) * 0.8 + 0.1).astype(np.float32)
+    out, st = run_both(nssb, img, dev, step, group, rng_)
+    assert st.timeouts == 0
+    assert_equal_lists(out)
+    assert st.refs == grid(w, 8, step) * grid(h, 8, step)
