@@ -81,7 +81,7 @@ __host__ __device__ inline TcwLayout tcw_layout(int N, int K) {
     const int ring_end = L.b_lo + (kRing + 1) * L.blk;
     const int scratch_end = L.b_hi + kWRefs * K * 8;  // list merges reuse the ring
     L.rs = ring_end > scratch_end ? ring_end : scratch_end;
-    L.ncb = L.rs + kRing * N * 4;
+    L.ncb = L.rs + kRing * N * 8;
     L.spos = L.ncb + 4 * N * 4;                 // uint16 [kCap][256] buffered survivors (row << 8 | column)
     L.se = L.spos + kCap * kWThreads * 2;        // float [kCap][256] their d~ - |r'|^2, then d
     L.wl = L.se + kCap * kWThreads * 4;          // uint16 [8 warps][32 * kCap] a warp's survivors in order
@@ -276,32 +276,34 @@ __global__ void __launch_bounds__(kWThreads, (K <= 15 ? 2 : 1))
 
     // image row r of the tile (Y = ylo + r) into ring slot r % kRing: candidate
     // column n's 8 shifted pixels as column n of the block, hi and lo, and
-    // their sum of squares (the row's share of candidate n's norm)
+    // their sum of squares (the row's share of candidate n's norm); two
+    // threads per column, four pixels each
     auto convert = [&](int r) {
         if (r >= nrows) return;
         const int slot = r % kRing;
         const float* rowp = src + (int64_t)(ylo + r) * ss;
-        for (int n = tid; n < N; n += kWThreads) {
-            float v[8];
+        for (int e = tid; e < 2 * N; e += kWThreads) {
+            const int n = e >> 1, h = e & 1;
+            float v[4];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int x = X0 + n + q;
+            for (int q = 0; q < 4; ++q) {
+                const int x = X0 + n + 4 * h + q;
                 v[q] = x < W ? __fsub_rn(__ldg(rowp + x), mu) : 0.f;
             }
             float sq = 0.f;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) sq = __fmaf_rn(v[q], v[q], sq);
-            rs[slot * N + n] = sq;
-            uint32_t hi[4], lo[4];
+            for (int q = 0; q < 4; ++q) sq = __fmaf_rn(v[q], v[q], sq);
+            rs[(slot * N + n) * 2 + h] = sq;
+            uint32_t hi[2], lo[2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) split2(v[2 * q], v[2 * q + 1], hi[q], lo[q]);
-            const int off = (n >> 3) * 128 + (n & 7) * 16;
-            const uint4 h4 = make_uint4(hi[0], hi[1], hi[2], hi[3]), l4 = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-            *reinterpret_cast<uint4*>(sm + L.b_hi + slot * L.blk + off) = h4;
-            *reinterpret_cast<uint4*>(sm + L.b_lo + slot * L.blk + off) = l4;
+            for (int q = 0; q < 2; ++q) split2(v[2 * q], v[2 * q + 1], hi[q], lo[q]);
+            const int off = (n >> 3) * 128 + (n & 7) * 16 + 8 * h;
+            const uint2 h2 = make_uint2(hi[0], hi[1]), l2 = make_uint2(lo[0], lo[1]);
+            *reinterpret_cast<uint2*>(sm + L.b_hi + slot * L.blk + off) = h2;
+            *reinterpret_cast<uint2*>(sm + L.b_lo + slot * L.blk + off) = l2;
             if (slot == 0) {
-                *reinterpret_cast<uint4*>(sm + L.b_hi + kRing * L.blk + off) = h4;
-                *reinterpret_cast<uint4*>(sm + L.b_lo + kRing * L.blk + off) = l4;
+                *reinterpret_cast<uint2*>(sm + L.b_hi + kRing * L.blk + off) = h2;
+                *reinterpret_cast<uint2*>(sm + L.b_lo + kRing * L.blk + off) = l2;
             }
         }
     };
@@ -311,7 +313,10 @@ __global__ void __launch_bounds__(kWThreads, (K <= 15 ? 2 : 1))
         for (int n = tid; n < N; n += kWThreads) {
             float s = 0.f;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) s += rs[((c + i) % kRing) * N + n];
+            for (int i = 0; i < 8; ++i) {
+                const float2 p = *reinterpret_cast<const float2*>(rs + (((c + i) % kRing) * N + n) * 2);
+                s += p.x + p.y;
+            }
             ncb[(c & 3) * N + n] = s;
         }
     };
@@ -378,13 +383,16 @@ __global__ void __launch_bounds__(kWThreads, (K <= 15 ? 2 : 1))
                 if (y == cy && self_col >= col0 && self_col < col0 + 16) m &= ~(1u << (self_col - col0));
                 float e[16];
                 if (m) {
+                    const float2 m2 = make_float2(-2.f, -2.f);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const float4 f = *reinterpret_cast<const float4*>(ncrow + col0 + 4 * q);
-                        e[4 * q] = __fmaf_rn(-2.f, D[4 * q], f.x);
-                        e[4 * q + 1] = __fmaf_rn(-2.f, D[4 * q + 1], f.y);
-                        e[4 * q + 2] = __fmaf_rn(-2.f, D[4 * q + 2], f.z);
-                        e[4 * q + 3] = __fmaf_rn(-2.f, D[4 * q + 3], f.w);
+                        const float2 a = __ffma2_rn(make_float2(D[4 * q], D[4 * q + 1]), m2, make_float2(f.x, f.y));
+                        const float2 b = __ffma2_rn(make_float2(D[4 * q + 2], D[4 * q + 3]), m2, make_float2(f.z, f.w));
+                        e[4 * q] = a.x;
+                        e[4 * q + 1] = a.y;
+                        e[4 * q + 2] = b.x;
+                        e[4 * q + 3] = b.y;
                     }
                 }
                 chunk(y, col0, m, e);
@@ -496,9 +504,16 @@ __global__ void __launch_bounds__(kWThreads, (K <= 15 ? 2 : 1))
         ok = sweep([&](int y, int col0, uint32_t m, const float* e) {
             uint32_t pm = 0;
             if (m) {
+                // most chunks hold no survivor: their smallest d~ decides
+                float mn = kInf;
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
-                    if (((m >> j) & 1u) && (flagged || e[j] <= th_e)) pm |= 1u << j;
+                    if ((m >> j) & 1u) mn = fminf(mn, e[j]);
+                if (flagged || mn <= th_e) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (((m >> j) & 1u) && (flagged || e[j] <= th_e)) pm |= 1u << j;
+                }
             }
             if (__any_sync(0xffffffffu, nbuf + __popc(pm) > kCap)) flush();
             if (pm) {
