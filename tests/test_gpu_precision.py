@@ -200,3 +200,17 @@ def test_large_window_small_and_thin_planes(nssb, synth, dev, w, h, step, rng_, 
     assert st.timeouts == 0
     assert_equal_lists(out)
     assert st.refs == grid(w, 8, step) * grid(h, 8, step)
+
+
+def test_uncovered_shapes_are_rejected(nssb, dev):
+    # the precision entry point covers 8x8 blocks at bm_range 9 (groups 2-16) and 10-64 (groups 2-32)
+    w, h = 64, 48
+    plane = torch.zeros((h, w), dtype=torch.float32, device=dev)
+    pos = torch.empty((grid(w, 8, 8) * grid(h, 8, 8), 32), dtype=torch.int32, device=dev)
+    cnt = torch.empty(grid(w, 8, 8) * grid(h, 8, 8), dtype=torch.int32, device=dev)
+    for rng_, group in ((65, 8), (9, 32), (40, 3), (5, 8)):
+        rc = nssb.lib().nssb_match_spatial_tc(plane.data_ptr(), w, w, h, 8, rng_, group, pos.data_ptr(), None,
+                                              cnt.data_ptr(), None, None)
+        assert rc != 0
+        with pytest.raises(nssb.Error, match="precision matcher covers"):
+            nssb.check(rc)
