@@ -212,6 +212,20 @@ def test_frame_api_chroma(nssb, oracle, synth, dev):
         assert oracle.psnr(both[c], want[c]) >= MIN_PSNR
 
 
+def test_frame_api_rgb(nssb, oracle, synth, dev):
+    # RGB: three full-resolution planes, each matched and filtered on its own,
+    # per-plane sigma; one and two stages against the oracle
+    planes = [synth.gray_frame(40 + c, 96, 72, sigma=8)[0] for c in range(3)]
+    clip = nssb.Clip.from_frames([tuple(planes)], nssb.RGB)
+    sig = [8.0, 5.0, 11.0]
+    one = nssb.BM3D(clip, sigma=sig).get_frame(0)
+    two = nssb.BM3D(clip, sigma=sig, final=1).get_frame(0)
+    for c in range(3):
+        st = oracle.stage(oracle.effective_sigma(sig[c]))
+        assert oracle.psnr(one[c], oracle.bm3d_plane(planes[c], st)) >= MIN_PSNR
+        assert oracle.psnr(two[c], oracle.bm3d_plane_two_stage(planes[c], st, st)[0]) >= MIN_PSNR
+
+
 def test_stage_errors_vs_fp64(nssb, oracle, dev):
     """Each stage against an FP64 host recomputation of the same groups."""
     import importlib
