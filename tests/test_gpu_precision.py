@@ -189,6 +189,16 @@ def test_automatic_matcher_form(nssb, synth, dev):
         assert (st.tc_refs > 0) == tensor
         auto.close()
         fp32.close()
+    # temporal: the centre frame's spatial matching takes the same choice
+    tclip = nssb.Clip.from_frames(synth.panning_clip(32, 160, 96, frames=3, sigma=10), nssb.YUV, 1, 1)
+    auto, fp32 = (nssb.BM3D(tclip, sigma=10, radius=1, final=1, bm_range=40) for _ in range(2))
+    fp32.set_matcher(0)
+    auto.stats(True, True)
+    for n in range(3):
+        assert all(np.array_equal(x, y) for x, y in zip(auto.get_frame(n), fp32.get_frame(n)))
+    assert auto.stats(False, False).tc_refs > 0
+    auto.close()
+    fp32.close()
 
 
 @pytest.mark.parametrize("w,h", [(8, 8), (9, 40), (40, 9), (300, 8), (13, 200), (71, 67)])
