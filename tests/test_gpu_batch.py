@@ -154,3 +154,27 @@ def test_batch_rejects(nssb, synth, dev):
     with pytest.raises(nssb.Error, match="radius-0"):
         b.run([(t, 1)])
     b.close()
+
+
+def test_plan_reused_for_other_nodes_of_equal_arguments(nssb, synth, dev):
+    # A batch plan laid out for one node serves any later node with the same
+    # arguments; the first node may be gone by then (the serving form retires
+    # requests every tick), so the plan must take every stage parameter from
+    # the items of the run in hand, not from the node it was laid out for.
+    frames = [(synth.gray_frame(70 + i, 96, 64, 10)[0],) for i in range(2)]
+    batch = nssb.Batch()
+    first = nssb.BM3D(nssb.Clip.from_frames(frames, nssb.GRAY), sigma=10, final=1)
+    batch.run([(first, 0)])
+    first.close()
+    # other nodes (other block sizes, ranges, groups) take the memory the first one released
+    others = [nssb.BM3D(nssb.Clip.from_frames(frames, nssb.GRAY), sigma=s, block_size=b, bm_range=r,
+                        group_size=g) for s, b, r, g in ((3, 4, 5, 4), (20, 16, 7, 16), (7, 12, 4, 2), (9, 8, 3, 32))]
+    second = nssb.BM3D(nssb.Clip.from_frames(frames, nssb.GRAY), sigma=10, final=1)
+    for n in range(2):
+        got = batch.run([(second, n)])[0]
+        want = second.get_frame(n)
+        assert all(np.array_equal(a, b) for a, b in zip(got, want))
+    for o in others:
+        o.close()
+    second.close()
+    batch.close()

@@ -151,7 +151,11 @@ std::string BatchPlan::signature_of(const BatchItem* items, int n) {
 
 void BatchPlan::layout(const BatchItem* items, int n, cudaStream_t stream) {
     std::string sig = signature_of(items, n);
-    if (arena_ && sig == sig_) return;
+    if (arena_ && sig == sig_) {
+        // the same layout: the arena stays, the stage lists point at this run's items
+        bind(items, n);
+        return;
+    }
     NSSB_CUDA(cudaSetDevice(device_));
     NSSB_CUDA(cudaStreamSynchronize(stream));  // the arena's previous layout is done with
     release_graph();
@@ -225,6 +229,19 @@ void BatchPlan::layout(const BatchItem* items, int n, cudaStream_t stream) {
         scratch_[k].count = reinterpret_cast<int32_t*>(arena_ + pl.count);
         scratch_[k].cube = F(pl.cube);
     }
+    bind(items, n);
+    sig_ = std::move(sig);
+}
+
+// The stage lists of the laid-out arena for these items: each plane's stage
+// parameters are the item's own (items of equal signatures have equal
+// values, but an earlier run's items may be gone).
+void BatchPlan::bind(const BatchItem* items, int n) {
+    for (int s = 0; s < 2; ++s) {
+        stage_[s].clear();
+        prematch_[s].clear();
+    }
+    auto F = [&](size_t o) { return o == kNone ? nullptr : reinterpret_cast<float*>(arena_ + o); };
     size_t k = 0;
     for (int i = 0; i < n; ++i) {
         const Bm3dConfig& c = *items[i].cfg;
@@ -250,7 +267,6 @@ void BatchPlan::layout(const BatchItem* items, int n, cudaStream_t stream) {
             }
         }
     }
-    sig_ = std::move(sig);
 }
 
 void BatchPlan::upload(const BatchItem* items, int n, cudaStream_t s) {

@@ -65,6 +65,7 @@ public:
     // Lays the batch out; keeps the arena (and graph) when the layout is
     // unchanged. A new layout first waits for the plan's work on `s`.
     void layout(const BatchItem* items, int n, cudaStream_t s);
+    void bind(const BatchItem* items, int n);
     static std::string signature_of(const BatchItem* items, int n);
     const std::string& signature() const { return sig_; }
     size_t arena_bytes() const { return arena_bytes_; }
