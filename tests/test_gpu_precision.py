@@ -224,3 +224,38 @@ def test_uncovered_shapes_are_rejected(nssb, dev):
         assert rc != 0
         with pytest.raises(nssb.Error, match="precision matcher covers"):
             nssb.check(rc)
+
+
+def test_automatic_form_in_cbm3d_batch_and_served(nssb, synth, dev):
+    # bm_range 40 takes the tensor form by default in every path that matches:
+    # CBM3D (plane 0's groups serve all planes), the batched form and the
+    # serving form -- each output equal to the FP32 form's bit for bit
+    rng = np.random.default_rng(9)
+    y = synth.gray_frame(51, 136, 96, 10)[0]
+    u = (y * 0.3 + rng.normal(0, 0.02, y.shape)).astype(np.float32)
+    v = (0.5 - y * 0.2 + rng.normal(0, 0.02, y.shape)).astype(np.float32)
+    c444 = nssb.Clip.from_frames([(y, u, v)], nssb.YUV, 0, 0)
+    auto = nssb.BM3D(c444, sigma=[10, 6, 6], chroma=1, final=1, bm_range=40)
+    fp32 = nssb.BM3D(c444, sigma=[10, 6, 6], chroma=1, final=1, bm_range=40)
+    fp32.set_matcher(0)
+    want = fp32.get_frame(0)
+    assert all(np.array_equal(a, b) for a, b in zip(auto.get_frame(0), want))
+    # the batched form (its autotuner may pick either matcher form) equals the node
+    frames = synth.yuv420_clip(52, 160, 96, 2, 10.0)
+    node = nssb.BM3D(nssb.Clip.from_frames(frames, nssb.YUV, 1, 1), sigma=10, final=1, bm_range=40)
+    batch = nssb.Batch()
+    got = batch.run([(node, 0), (node, 1), (auto, 0)])
+    assert all(np.array_equal(a, b) for a, b in zip(got[0], node.get_frame(0)))
+    assert all(np.array_equal(a, b) for a, b in zip(got[1], node.get_frame(1)))
+    assert all(np.array_equal(a, b) for a, b in zip(got[2], want))
+    batch.close()
+    # a served request
+    srv = nssb.Server(device_id=0, workers=2)
+    clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
+    outs = [tuple(np.empty_like(p) for p in f) for f in frames]
+    srv.wait(srv.submit(clip, outs=outs, sigma=10, final=1, bm_range=40))
+    srv.close()
+    for n in range(2):
+        assert all(np.array_equal(a, b) for a, b in zip(outs[n], node.get_frame(n)))
+    for x in (auto, fp32, node):
+        x.close()
