@@ -112,34 +112,6 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
                      ((reinterpret_cast<uintptr_t>(P.num) | reinterpret_cast<uintptr_t>(P.src) |
                        reinterpret_cast<uintptr_t>(P.dst)) & 15) == 0 &&
                      ((P.acc_stride | P.sstride | P.dstride) & 3) == 0;
-    long long* const np = P.num + (int64_t)y * P.acc_stride + xs;
-    float* const dp = P.dst + (int64_t)y * P.dstride + xs;
-    long long nv[8];
-    float sv[8];
-    if (vec) {
-        const float* sp = P.src + (int64_t)y * P.sstride + xs;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-            const longlong2 t = reinterpret_cast<const longlong2*>(np)[h];
-            nv[2 * h] = t.x;
-            nv[2 * h + 1] = t.y;
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(sp) + h);
-            sv[4 * h] = t.x;
-            sv[4 * h + 1] = t.y;
-            sv[4 * h + 2] = t.z;
-            sv[4 * h + 3] = t.w;
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const bool ok = xs + j < P.W && y < P.H;
-            nv[j] = ok ? np[j] : 0;
-            sv[j] = ok ? __ldg(P.src + (int64_t)y * P.sstride + xs + j) : 0.f;
-        }
-    }
     // vertical sums: quarter q, tile column c (vs column c + B - 1) and, for
     // c < B - 1, halo column c (vs column c)
     {
@@ -184,6 +156,34 @@ __global__ void __launch_bounds__(kFT) finish_batch_kernel(const __grid_constant
         }
     }
     __syncthreads();
+    long long* const np = P.num + (int64_t)y * P.acc_stride + xs;
+    float* const dp = P.dst + (int64_t)y * P.dstride + xs;
+    long long nv[8];
+    float sv[8];
+    if (vec) {
+        const float* sp = P.src + (int64_t)y * P.sstride + xs;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const longlong2 t = reinterpret_cast<const longlong2*>(np)[h];
+            nv[2 * h] = t.x;
+            nv[2 * h + 1] = t.y;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(sp) + h);
+            sv[4 * h] = t.x;
+            sv[4 * h + 1] = t.y;
+            sv[4 * h + 2] = t.z;
+            sv[4 * h + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const bool ok = xs + j < P.W && y < P.H;
+            nv[j] = ok ? np[j] : 0;
+            sv[j] = ok ? __ldg(P.src + (int64_t)y * P.sstride + xs + j) : 0.f;
+        }
+    }
     // horizontal sums along this thread's 8 pixels, then the finish
     const long long* row = vs + r * pitch;
     long long den = 0;
