@@ -178,10 +178,10 @@ void validate_numeric(const Args& args) {
     }
 }
 
-// parse_sigma (bm3d_args.cpp:17-25): `given` keeps the user values.
-void parse_sigma(const Args& args, int np, float sigma[3], float given[3]) {
+// parse_sigma (bm3d_args.cpp:17-25): `user_sigma` keeps the values as the caller gave them.
+void parse_sigma(const Args& args, int np, float sigma[3], float user_sigma[3]) {
     args.float_array("sigma", sigma, np, kDefaultSigma);
-    std::copy_n(sigma, 3, given);
+    std::copy_n(sigma, 3, user_sigma);
     for (int i = 0; i < np; ++i) {
         if (!finite_bits(sigma[i]) || sigma[i] < 0.f) fail("sigma must be finite and non-negative");
         if (sigma[i] != 0.f) sigma[i] = effective_sigma(sigma[i]);
@@ -227,11 +227,11 @@ void parse_chroma(const Args& args, const nssb_video_info& vi, Parsed& p) {
 
 // parse_basic_stage (bm3d_args.cpp:61-96)
 void parse_basic(const Args& args, const nssb_video_info& vi, bool sigma_basic, bool block_basic, bool group_basic,
-                 float given[3], Parsed& p) {
+                 float user_sigma[3], Parsed& p) {
     const int np = num_planes(vi);
-    if (sigma_basic) args.float_array("sigma_basic", given, np, kDefaultSigma);
-    const bool step_given = args.count("block_step") > 0;
-    const bool ps_given = args.count("ps_num") > 0;
+    if (sigma_basic) args.float_array("sigma_basic", user_sigma, np, kDefaultSigma);
+    const bool has_block_step = args.count("block_step") > 0;
+    const bool has_ps_num = args.count("ps_num") > 0;
     for (int i = 0; i < np; ++i) {
         p.block_basic[i] = p.block[i];
         p.group_basic[i] = p.group[i];
@@ -239,17 +239,17 @@ void parse_basic(const Args& args, const nssb_video_info& vi, bool sigma_basic, 
     if (block_basic) args.inherit_int("block_size_basic", p.block_basic, np, kDefaultBlock);
     if (group_basic) args.inherit_int("group_size_basic", p.group_basic, np, kDefaultGroup);
     for (int i = 0; i < np; ++i) {
-        const int plane = p.chroma ? 0 : i;
-        p.block_basic[i] = p.block_basic[plane];
-        p.group_basic[i] = p.group_basic[plane];
-        if (!finite_bits(given[i]) || given[i] < 0.f) fail("sigma_basic must be finite and non-negative");
-        p.sigma_basic[i] = given[i] != 0.f ? effective_sigma(given[i]) : 0.f;
+        const int source = p.chroma ? 0 : i;  // CBM3D: every plane takes plane 0's shape
+        p.block_basic[i] = p.block_basic[source];
+        p.group_basic[i] = p.group_basic[source];
+        if (!finite_bits(user_sigma[i]) || user_sigma[i] < 0.f) fail("sigma_basic must be finite and non-negative");
+        p.sigma_basic[i] = user_sigma[i] != 0.f ? effective_sigma(user_sigma[i]) : 0.f;
         if (!allowed_block(p.block_basic[i])) fail("block_size_basic must be one of 1, 2, 4, 8, 12, 16, 32");
         if (!allowed_group(p.group_basic[i])) fail("group_size_basic must be one of 1, 2, 4, 8, 16, 32, 64");
         if (p.block_basic[i] > plane_width(vi, i) || p.block_basic[i] > plane_height(vi, i))
             fail("block_size_basic must not exceed plane dimensions");
-        p.step_basic[i] = step_given ? p.step[i] : std::min(kDefaultStep, p.block_basic[i]);
-        p.ps_num_basic[i] = ps_given ? p.ps_num[i] : std::min(kDefaultPsNum, p.group_basic[i]);
+        p.step_basic[i] = has_block_step ? p.step[i] : std::min(kDefaultStep, p.block_basic[i]);
+        p.ps_num_basic[i] = has_ps_num ? p.ps_num[i] : std::min(kDefaultPsNum, p.group_basic[i]);
         if (p.step_basic[i] > p.block_basic[i]) fail("block_step must be in [1, block_size_basic]");
         if (p.ps_num_basic[i] > p.group_basic[i]) fail("ps_num must be in [1, group_size_basic]");
     }
@@ -275,8 +275,8 @@ Parsed parse_bm3d(const Args& args, const nssb_video_info& vi, const nssb_video_
     if (ref && !same_video(vi, *ref)) fail("ref must match clip");
     Parsed p;
     const int np = num_planes(vi);
-    float given[3];
-    parse_sigma(args, np, p.sigma, given);
+    float user_sigma[3];
+    parse_sigma(args, np, p.sigma, user_sigma);
     args.inherit_int("block_size", p.block, np, kDefaultBlock);
     args.inherit_int("group_size", p.group, np, kDefaultGroup);
     map_adaptive(args, "block_step", p.step, np, kDefaultStep, p.block);
@@ -295,7 +295,7 @@ Parsed parse_bm3d(const Args& args, const nssb_video_info& vi, const nssb_video_
     if (!p.final && (sigma_basic || block_basic || group_basic))
         fail("sigma_basic, block_size_basic and group_size_basic require final=1");
     if (p.final && ref) fail("use only one of final and ref");
-    if (p.final) parse_basic(args, vi, sigma_basic, block_basic, group_basic, given, p);
+    if (p.final) parse_basic(args, vi, sigma_basic, block_basic, group_basic, user_sigma, p);
     check_planes(vi, p);
     return p;
 }
