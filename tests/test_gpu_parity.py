@@ -154,6 +154,43 @@ def test_stage_vs_oracle(nssb, oracle, synth, dev, block, step, group, rng_, wie
     assert np.array_equal(got, gpu_stage(nssb, noisy, ref, st, dev))  # run-to-run identical
 
 
+def stage_at(nssb, src, ref, dev, pitch, offset, sigma):
+    """nssb_bm3d_plane_stage (8x8 blocks, groups of 8, step 8, bm_range 9) on
+    planes laid out at `pitch` floats per row, `offset` floats into their
+    allocation."""
+    h, w = src.shape
+
+    def place(a):
+        buf = torch.zeros(offset + h * pitch, dtype=torch.float32, device=dev)
+        if a is not None:
+            buf[offset:].view(h, pitch)[:, :w] = to_dev(a, dev)
+        return buf
+
+    s, o = place(src), place(None)
+    r = place(ref) if ref is not None else None
+    ptr = lambda t: t.data_ptr() + 4 * offset
+    nssb.check(nssb.lib().nssb_bm3d_plane_stage(ptr(s), ptr(r) if r is not None else None, ptr(o), pitch, w, h,
+                                                sigma, 8, 8, 8, 9, None))
+    torch.cuda.synchronize()
+    return o[offset:].view(h, pitch)[:, :w].cpu().numpy()
+
+
+@pytest.mark.parametrize("w,h", [(96, 64), (240, 136), (1920, 1080)])
+def test_staged_rows_equal_plane_reads(nssb, oracle, synth, dev, w, h):
+    """The group filter reads patch rows as aligned 16-byte chunks when the
+    plane's rows start on 16 bytes and one float at a time otherwise (an odd
+    pitch, a base 4 bytes off); the matcher and the finish take any pitch:
+    the same bits for every layout, in both stages."""
+    noisy, _ = synth.gray_frame(17, w, h, sigma=10)
+    sigma = oracle.effective_sigma(10.0)
+    basic = stage_at(nssb, noisy, None, dev, w, 0, sigma)
+    for pitch, offset in ((w + 1, 0), (w, 1), (w + 4, 0)):
+        assert np.array_equal(basic, stage_at(nssb, noisy, None, dev, pitch, offset, sigma)), (pitch, offset)
+    final = stage_at(nssb, noisy, basic, dev, w, 0, sigma)
+    for pitch, offset in ((w + 1, 0), (w, 1), (w + 4, 0)):
+        assert np.array_equal(final, stage_at(nssb, noisy, basic, dev, pitch, offset, sigma)), (pitch, offset)
+
+
 def test_frame_api_two_stage_yuv420(nssb, oracle, synth, dev):
     frames = synth.yuv420_clip(3, 128, 96, frames=2, sigma=5)
     clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
