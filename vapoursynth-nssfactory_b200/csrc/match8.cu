@@ -239,8 +239,11 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     const int cpw = (ncols + P - 1) / P;
     const int d0 = (banded ? 0 : R - Rr) + part * cpw, d1 = min((banded ? 0 : R - Rr) + ncols, d0 + cpw);
     const bool down = !banded && d1 - 1 <= R;
+    // one part: the centre column, then outwards on alternate sides (R - 1,
+    // R + 1, R - 2, ...), so the list's threshold tightens from both sides
+    const bool alt = P == 1 && !banded;
     for (int m = 0; m < d1 - d0; ++m) {
-        const int dxi = down ? d1 - 1 - m : d0 + m;
+        const int dxi = alt ? R + ((m & 1) ? -((m + 1) >> 1) : (m >> 1)) : down ? d1 - 1 - m : d0 + m;
         const int x = cx + ox + dxi;
         const bool xok = x >= left && x <= right;
         Mask pass = 0;
