@@ -114,9 +114,10 @@ struct SplitTopK {
 
 constexpr int kLanes = 32;   // references per CTA
 // tile row pitch: the 31 * 8 + 2R + 8 columns of 32 references at step <= 8,
-// rounded up to whole 32-column groups (288 for ranges up to 15)
+// rounded up to a multiple of 4 (the swizzle only permutes a column within
+// its aligned group of 4; 276 floats at range 9)
 template <int R>
-__host__ __device__ constexpr int tile_pitch() { return (31 * 8 + 2 * R + 8 + 31) / 32 * 32; }
+__host__ __device__ constexpr int tile_pitch() { return (31 * 8 + 2 * R + 8 + 3) / 4 * 4; }
 
 template <int R>
 __host__ __device__ constexpr int tile_rows() { return 2 * R + 8; }
@@ -185,7 +186,11 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
     // finished distances of the current column, one slot per candidate row:
     // an emit stores its sum and marks a bit when it may enter the list; the
     // insertions run after the column, once per marked candidate
-    float* stash = tile + TR * kPitch + threadIdx.x;  // [NC][blockDim]
+    // one slot per reference and candidate row of the part's current column:
+    // a reference's two lanes hold the same sum (their halves meet in one
+    // commutative add), so both store it to the same slot and each reads
+    // back its own store
+    float* stash = tile + TR * kPitch + part * (NC * kLanes) + l;  // [P][NC][32 references]
     const float2 neg1 = make_float2(-1.f, -1.f);
     for (int band = 0; band < nb * nb; ++band) {
     // candidate (band column d, band row k) is (cx + ox + d, cy + oy + k)
@@ -282,7 +287,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
                 acc[ks][0] = acc[ks][1] = make_float2(0.f, 0.f);
                 const float half_sum = __fadd_rn(__fadd_rn(a.x, a.y), __fadd_rn(b.x, b.y));
                 const float dd = __fadd_rn(half_sum, __shfl_xor_sync(0xffffffffu, half_sum, 16));
-                stash[kd * (64 * P)] = dd;
+                stash[kd * kLanes] = dd;
                 pass |= Mask(dd > worst ? 0 : 1) << kd;
             }
         };
@@ -312,7 +317,7 @@ __device__ __forceinline__ void match8_tile(const MatchBatch& mb, int tile_id, f
         while (pass) {
             const int kd = first_bit(pass);
             pass &= pass - 1;
-            topk.add(key_of(stash[kd * (64 * P)], x, cy + oy + kd));
+            topk.add(key_of(stash[kd * kLanes], x, cy + oy + kd));
         }
     }
     }  // bands
@@ -389,7 +394,7 @@ void launch_rkp(MatchBatch& mb, const MatchTune& tune, cudaStream_t stream) {
     mb.queue = nullptr;
     if (ctas == 0) return;
     static_assert(2 * R + 1 <= 64, "a column's candidates must fit the row mask");
-    const size_t smem = std::max((size_t)(tile_pitch<R>() * tile_rows<R>() + (2 * R + 1) * 64 * P) * sizeof(float),
+    const size_t smem = std::max((size_t)(tile_pitch<R>() * tile_rows<R>() + (2 * R + 1) * kLanes * P) * sizeof(float),
                                  (size_t)P * K * kLanes * sizeof(uint64_t));
     auto kern = match8_kernel<R, K, P, BANDED>;
     NSSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
