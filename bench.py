@@ -500,8 +500,9 @@ def heavy_only(nssb, synth, dev, args):
 def wide_window_leg(nssb, synth, dev, n_frames=4):
     """The precision form at large search windows against the FP32 matchers:
     the reference's "heavy" preset (final=1, block_step=3, group_size=32,
-    group_size_basic=16, bm_range=19) and final=1 at bm_range 25, 31, 40 and
-    64 (step 8) and 40 (step 4) on
+    group_size_basic=16, bm_range=19) and final=1 at bm_range 25, 31, 40, 48,
+    56 and 64 (step 8) and 40 (steps 4, 6 and 7: where the automatic form
+    switches) on
     1080p YUV420 frames of the headline generator; per-frame drop-in, matcher
     time per frame (CUDA events around each matching launch), whole frames/s,
     outputs compared bit for bit between the forms."""
@@ -512,7 +513,10 @@ def wide_window_leg(nssb, synth, dev, n_frames=4):
     shapes = {"heavy": dict(final=1, block_step=3, group_size=32, group_size_basic=16, bm_range=19),
               "bm_range_25": dict(final=1, bm_range=25), "bm_range_31": dict(final=1, bm_range=31),
               "bm_range_40": dict(final=1, bm_range=40), "bm_range_64": dict(final=1, bm_range=64),
-              "bm_range_40_step_4": dict(final=1, bm_range=40, block_step=4)}
+              "bm_range_40_step_4": dict(final=1, bm_range=40, block_step=4),
+              "bm_range_48": dict(final=1, bm_range=48), "bm_range_56": dict(final=1, bm_range=56),
+              "bm_range_40_step_6": dict(final=1, bm_range=40, block_step=6),
+              "bm_range_40_step_7": dict(final=1, bm_range=40, block_step=7)}
     res = {}
     for name, kw in shapes.items():
         outs, row = {}, {}

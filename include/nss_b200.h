@@ -151,7 +151,8 @@ int nssb_bm3d_stats(nssb_bm3d* h, int enable_timing, int reset, nssb_kernel_stat
 /* Matcher of a handle's 8x8 stages (spatial and the centre frame of
  * temporal): 0 = FP32, 1 = the tensor-core precision form of
  * nssb_match_spatial_tc, 2 = automatic (the default): the precision form
- * from bm_range 32 on, where it measured faster, FP32 below. Outputs are
+ * where it measured faster -- from bm_range 32 on at block steps 1-7, from
+ * 63 on at step 8 -- and FP32 elsewhere. Outputs are
  * bit-identical whichever form runs. No reference counterpart (the
  * reference picks its CUDA matcher by shape, src/cuda/common/match.cu:1605-1611). */
 #define NSSB_MATCHER_FP32 0

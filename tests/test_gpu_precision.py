@@ -175,12 +175,13 @@ def test_heavy_preset_1080p_plane(nssb, synth, dev):
 
 
 def test_automatic_matcher_form(nssb, synth, dev):
-    # the default form takes the precision form from bm_range 32 on and the FP32 matcher below;
-    # the output is the FP32 form's bit for bit either way
+    # the default form takes the precision form from bm_range 32 on at block steps 1-7 and
+    # from 63 on at step 8, the FP32 matcher otherwise; the output is the FP32 form's bit
+    # for bit either way
     frames = synth.yuv420_clip(31, 256, 144, 1, 10.0)
     clip = nssb.Clip.from_frames(frames, nssb.YUV, 1, 1)
-    for rng_, tensor in ((40, True), (16, False)):
-        auto, fp32 = nssb.BM3D(clip, sigma=10, final=1, bm_range=rng_), nssb.BM3D(clip, sigma=10, final=1, bm_range=rng_)
+    for rng_, step, tensor in ((40, 8, False), (64, 8, True), (40, 4, True), (16, 4, False)):
+        auto, fp32 = (nssb.BM3D(clip, sigma=10, final=1, bm_range=rng_, block_step=step) for _ in range(2))
         fp32.set_matcher(0)
         auto.stats(True, True)
         a, b = auto.get_frame(0), fp32.get_frame(0)
@@ -191,7 +192,7 @@ def test_automatic_matcher_form(nssb, synth, dev):
         fp32.close()
     # temporal: the centre frame's spatial matching takes the same choice
     tclip = nssb.Clip.from_frames(synth.panning_clip(32, 160, 96, frames=3, sigma=10), nssb.YUV, 1, 1)
-    auto, fp32 = (nssb.BM3D(tclip, sigma=10, radius=1, final=1, bm_range=40) for _ in range(2))
+    auto, fp32 = (nssb.BM3D(tclip, sigma=10, radius=1, final=1, bm_range=64) for _ in range(2))
     fp32.set_matcher(0)
     auto.stats(True, True)
     for n in range(3):

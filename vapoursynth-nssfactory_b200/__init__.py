@@ -325,7 +325,8 @@ class Node:
 
     def set_matcher(self, form: int) -> None:
         """0: FP32 matcher; 1: tensor-core precision form; 2: automatic (the default: the precision
-        form from bm_range 32 on, FP32 below). Identical lists whichever runs."""
+        form from bm_range 32 on at block steps 1-7 and from 63 on at step 8, FP32 elsewhere).
+        Identical lists whichever runs."""
         check(lib().nssb_bm3d_set_matcher(self.handle, int(form)))
 
     def set_window(self, beta: float) -> None:

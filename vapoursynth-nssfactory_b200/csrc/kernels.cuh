@@ -72,12 +72,19 @@ struct TcCounters {
     unsigned long long survivors, refs;
     unsigned int max_ratio_bits, flagged_tiles, timeouts, pad;
 };
-// Whether a stage of 8x8 blocks with this search range takes the precision
-// form: asked for (form 1), or automatically (form 2) from bm_range 32 on,
-// where the FP32 matcher sweeps the window in bands and the tensor form
-// measured 1.3-2.8x faster on 1080p YUV420 frames (steps 3-8, ranges 32-64;
-// below range 32 the FP32 matchers are faster). Lists are identical either way.
-inline bool tensor_matcher_takes(int form, int bm_range) { return form == 1 || (form == 2 && bm_range >= 32); }
+// Whether a stage of 8x8 blocks with this search range and block step takes
+// the precision form: asked for (form 1), or automatically (form 2) where it
+// measured faster on 1080p YUV420 frames. Beyond range 31 the FP32 matcher
+// sweeps the window in bands of 63 x 63 candidates, its time growing with
+// (2R + 1) x the number of row bands; the tensor form's grows with 2R + 1 and
+// shares more candidate columns between references at smaller steps. At
+// steps 1-7 the tensor form wins from range 32 (range 40: 1.15x at step 7,
+// 1.18x at step 6, 1.58x at step 4); at step 8 only from range 63, where the
+// FP32 matcher needs a third row band (1.46x at range 64; at ranges 40-56 it
+// is 2-8 % faster itself). Lists are identical either way.
+inline bool tensor_matcher_takes(int form, int bm_range, int step) {
+    return form == 1 || (form == 2 && bm_range >= (step >= 8 ? 63 : 32));
+}
 // The precision form: bm_range 9 on match_tc.cu's kernel, 10-64 on match_tcw.cu's
 // (references on the MMA's M side); false where neither covers the shape.
 bool launch_match_tc_batch(MatchBatch& batch, int bm_range, int group, TcCounters* counters, cudaStream_t stream);

@@ -59,7 +59,7 @@ void run_set(const StagePlane* planes, const int* set, int ns, cudaStream_t stre
         bool ok = false;
         if (sp.block == 8) {
             clock.begin(StageClock::kMatch);
-            if (tensor_matcher_takes(tunes.match.form, sp.bm_range) && tunes.match.tc)
+            if (tensor_matcher_takes(tunes.match.form, sp.bm_range, sp.step) && tunes.match.tc)
                 ok = launch_match_tc_batch(mb, sp.bm_range, sp.group, tunes.match.tc, stream);
             if (!ok) cleared = ok = launch_match8_batch(mb, sp.bm_range, sp.group, stream, &tunes.match);
             clock.end(StageClock::kMatch);

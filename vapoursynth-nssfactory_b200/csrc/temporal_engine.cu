@@ -242,7 +242,7 @@ private:
                     mbatch_.p[q] = MatchPlane{tps[q].plane[r_], tps[q].stride[r_], pos_[mp], dist_[mp], count_[mp],
                                               cfg_.plane_w[mp], cfg_.plane_h[mp], 0, 0, 0};
                 }
-                if (tune_ && tensor_matcher_takes(tune_->form, m0.bm_range) && tune_->tc)
+                if (tune_ && tensor_matcher_takes(tune_->form, m0.bm_range, m0.step) && tune_->tc)
                     done = launch_match_tc_batch(mbatch_, m0.bm_range, m0.group, tune_->tc, stream_);
                 if (!done) done = launch_match8_batch(mbatch_, m0.bm_range, m0.group, stream_);
             }
